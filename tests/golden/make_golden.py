@@ -1,0 +1,167 @@
+"""Generates the golden fixtures in this folder from the reference KSig itself.
+
+Run from the repository root, in a container that has the reference source
+checked out at ``--ref`` (default ``/root/reference``)::
+
+    python tests/golden/make_golden.py [--ref /root/reference]
+
+The reference needs CuPy and a CUDA device.  Neither is needed here: the
+NumPy-backed ``cupy`` stand-in in ``tests/_refshim`` takes CuPy's place and
+Numba's CUDA simulator (``NUMBA_ENABLE_CUDASIM=1``) runs the Numba PDE kernel
+of ksig/algorithms.py:344-399 unchanged.  Every case stores its inputs, its
+parameters and the reference's outputs in ``golden.npz``; the tests read only
+that file, never the reference.
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SHIM = os.path.join(os.path.dirname(HERE), '_refshim')
+
+
+def _cases():
+  import numpy as np
+  cases = []
+
+  def add(name, kernel, params, X, Y=None, ragged=False):
+    cases.append(dict(name=name, kernel=kernel, params=params, X=X, Y=Y,
+                      ragged=ragged))
+
+  rng = np.random.default_rng(0)
+  X0 = rng.standard_normal((10, 50, 5))
+  Y0 = rng.standard_normal((8, 20, 5))
+  base = dict(n_levels=5, order=1, normalize=False, static='rbf', param=1.0)
+  add('cfg1_dp_rbf', 'sig', base, X0, Y0)
+  add('cfg1_dp_rbf_norm', 'sig', dict(base, normalize=True), X0, Y0)
+
+  rng = np.random.default_rng(10)
+  X1 = np.cumsum(rng.standard_normal((6, 17, 3)) * 0.3, axis=1)
+  Y1 = np.cumsum(rng.standard_normal((5, 13, 3)) * 0.3, axis=1)
+  add('dp_o2_m4', 'sig', dict(n_levels=4, order=2, normalize=False,
+                               static='rbf', param=0.7), X1, Y1)
+  add('dp_o2_m4_norm', 'sig', dict(n_levels=4, order=2, normalize=True,
+                                    static='rbf', param=0.7), X1, Y1)
+  add('dp_o3_m5', 'sig', dict(n_levels=5, order=3, normalize=False,
+                               static='rbf', param=1.3), X1, Y1)
+  add('dp_ofull_m3', 'sig', dict(n_levels=3, order=0, normalize=False,
+                                  static='rbf', param=1.0), X1, Y1)
+  add('dp_linear', 'sig', dict(n_levels=4, order=1, normalize=False,
+                                static='linear', param=0.5), X1, Y1)
+  add('dp_linear_norm', 'sig', dict(n_levels=4, order=1, normalize=True,
+                                     static='linear', param=0.5), X1, Y1)
+  add('dp_nodiff', 'sig', dict(n_levels=3, order=1, normalize=False,
+                                difference=False, static='rbf', param=2.0),
+      X1[:, :9], Y1[:, :7])
+  add('dp_m1', 'sig', dict(n_levels=1, order=1, normalize=True,
+                            static='rbf', param=1.0), X1, Y1)
+  rng = np.random.default_rng(11)
+  add('dp_d1_L2', 'sig', dict(n_levels=3, order=1, normalize=False,
+                               static='rbf', param=1.0),
+      rng.standard_normal((4, 2, 1)), rng.standard_normal((3, 2, 1)))
+  add('dp_L1', 'sig', dict(n_levels=3, order=1, normalize=False,
+                            static='rbf', param=1.0),
+      rng.standard_normal((3, 1, 2)), rng.standard_normal((2, 5, 2)))
+
+  # Ragged batch pinned through the reference's padding invariance: the
+  # reference sees edge-padded dense arrays, the fixture keeps the lengths.
+  rng = np.random.default_rng(12)
+  lens_x = [7, 12, 3, 9]
+  lens_y = [5, 12, 10]
+  xs = [np.cumsum(rng.standard_normal((n, 2)) * 0.4, axis=0) for n in lens_x]
+  ys = [np.cumsum(rng.standard_normal((n, 2)) * 0.4, axis=0) for n in lens_y]
+  add('dp_ragged_o1', 'sig', dict(n_levels=4, order=1, normalize=True,
+                                   static='rbf', param=0.8), xs, ys,
+      ragged=True)
+  add('dp_ragged_o2', 'sig', dict(n_levels=4, order=2, normalize=False,
+                                   static='rbf', param=0.8), xs, ys,
+      ragged=True)
+
+  rng = np.random.default_rng(1)
+  A = rng.standard_normal((2, 8, 3))
+  B = rng.standard_normal((2, 6, 3))
+  add('pde_rbf', 'pde', dict(normalize=False, static='rbf', param=1.0), A, B)
+  add('pde_rbf_norm', 'pde', dict(normalize=True, static='rbf', param=1.0),
+      A, B)
+  rng = np.random.default_rng(13)
+  P = np.cumsum(rng.standard_normal((3, 9, 2)) * 0.5, axis=1)
+  Q = np.cumsum(rng.standard_normal((2, 11, 2)) * 0.5, axis=1)
+  add('pde_linear', 'pde', dict(normalize=False, static='linear', param=0.6),
+      P, Q)
+  add('pde_ragged', 'pde', dict(normalize=False, static='rbf', param=0.9),
+      [P[0, :5], P[1], P[2, :7]], [Q[0, :4], Q[1]], ragged=True)
+  return cases
+
+
+def _pad_edge(seqs):
+  import numpy as np
+  L = max(s.shape[0] for s in seqs)
+  return np.stack([np.concatenate([s, np.repeat(s[-1:], L - len(s), 0)], 0)
+                   for s in seqs])
+
+
+def _run_reference():
+  """Runs inside the shimmed interpreter; returns nothing, writes npz."""
+  import numba.cuda
+  numba.cuda.default_stream = lambda: 0
+  import numpy as np
+  import ksig
+  out = {}
+  meta = []
+  for c in _cases():
+    p = c['params']
+    static = (ksig.static.kernels.RBFKernel(p['param']) if p['static'] == 'rbf'
+              else ksig.static.kernels.LinearKernel(p['param']))
+    if c['kernel'] == 'sig':
+      K = ksig.kernels.SignatureKernel(
+          n_levels=p['n_levels'], order=p['order'],
+          difference=p.get('difference', True), normalize=p['normalize'],
+          static_kernel=static)
+    else:
+      K = ksig.kernels.SignaturePDEKernel(
+          difference=p.get('difference', True), normalize=p['normalize'],
+          static_kernel=static)
+    X, Y = c['X'], c['Y']
+    name = c['name']
+    if c['ragged']:
+      for i, s in enumerate(X):
+        out[f'{name}/X{i}'] = s
+      for i, s in enumerate(Y):
+        out[f'{name}/Y{i}'] = s
+      Xd, Yd = _pad_edge(X), _pad_edge(Y)
+      nx, ny = len(X), len(Y)
+    else:
+      out[f'{name}/X'] = X
+      out[f'{name}/Y'] = Y
+      Xd, Yd = X, Y
+      nx, ny = X.shape[0], Y.shape[0]
+    out[f'{name}/KXX'] = np.asarray(K(Xd))
+    out[f'{name}/KXY'] = np.asarray(K(Xd, Yd))
+    out[f'{name}/Kdiag'] = np.asarray(K(Xd, diag=True), dtype=np.float64)
+    meta.append(dict(name=name, kernel=c['kernel'], params=p,
+                     ragged=c['ragged'], nx=nx, ny=ny))
+  out['__meta__'] = np.array(json.dumps(meta))
+  np.savez_compressed(os.path.join(HERE, 'golden.npz'), **out)
+  print('wrote', len(meta), 'cases')
+
+
+def main():
+  ap = argparse.ArgumentParser()
+  ap.add_argument('--ref', default='/root/reference')
+  ap.add_argument('--_child', action='store_true')
+  a = ap.parse_args()
+  if a._child:
+    _run_reference()
+    return
+  env = dict(os.environ)
+  env['PYTHONPATH'] = os.pathsep.join([SHIM, a.ref])
+  env['NUMBA_ENABLE_CUDASIM'] = '1'
+  subprocess.run([sys.executable, '-W', 'ignore', os.path.abspath(__file__),
+                  '--_child'], env=env, check=True, cwd='/tmp')
+
+
+if __name__ == '__main__':
+  main()
