@@ -1,0 +1,369 @@
+"""Throughput of the fused signature-kernel Gram on B200.
+
+Workload (one step): the normalised truncated signature Gram K(X, Y) of
+N = M = 512 sequences per GPU, L = 200 points, d = 8 random-walk channels
+(cumsum of N(0, 1/L) increments) plus a linear time channel, RBF static
+kernel with bandwidth sqrt(8), n_levels = 5, order = 1, normalize = True,
+FP32 inputs (FP32 kernels with FP64 level sums and normalisation).  A step
+computes the 512 x 512 Gram plus the two 512-entry diagonal passes that
+normalisation needs, i.e. the whole ``SignatureKernel(...)(X, Y)`` call.
+
+Metric: Gram entries per second (N*M per step, summed over ranks).  With
+``--gpus N`` under torchrun every rank computes its own 512 x 512 block
+(weak scaling, no data-path collective).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+``--impl reference`` times the reference recursion on the host cores (the
+NumPy restatement in ``oracle/`` run over a process pool, since the
+reference itself needs CuPy on a GPU) on the same workload, one bounded
+sample of pairs per step.
+"""
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+  sys.path.insert(0, ROOT)
+
+N_SEQ = 512
+SEQ_LEN = 200
+D_WALK = 8
+N_LEVELS = 5
+ORDER = 1
+BANDWIDTH = math.sqrt(8.0)
+METRIC = 'Gram entries/sec & fwd+bwd s/step, mixed vs plain FP32 on B200 @1e-5 vs FP64'
+UNIT = 'Gram entries/s'
+WORKLOAD = 'sig_dp_rbf_N512_M512_L200_d9_m5_p1_normalized'
+
+
+def make_walks(n, L, d, seed):
+  """Random walks (cumsum of N(0, 1/L) increments) + a time channel."""
+  rng = np.random.default_rng(seed)
+  inc = rng.standard_normal((n, L - 1, d)) / np.sqrt(L)
+  X = np.concatenate([np.zeros((n, 1, d)), np.cumsum(inc, 1)], 1)
+  t = np.broadcast_to(np.linspace(0, 1, L)[None, :, None], (n, L, 1))
+  return np.concatenate([X, t], -1).astype(np.float32)
+
+
+def config(n_gpus, extra=None):
+  c = {'workload': WORKLOAD, 'n_x': N_SEQ, 'n_y': N_SEQ, 'seq_len': SEQ_LEN,
+       'd': D_WALK + 1, 'n_levels': N_LEVELS, 'order': ORDER,
+       'static_kernel': 'rbf', 'bandwidth': BANDWIDTH, 'normalize': True,
+       'global_pairs': N_SEQ * N_SEQ * n_gpus,
+       'parallelism': f'pairs-sharded x{n_gpus}' if n_gpus > 1 else 'single'}
+  if extra:
+    c.update(extra)
+  return c
+
+
+# ---------------------------------------------------------------------------
+# Host CPU baseline: the reference recursion restated in NumPy (oracle/).
+# ---------------------------------------------------------------------------
+
+def _cpu_chunk(args):
+  X, Y = args
+  sys.path.insert(0, ROOT)
+  from oracle import ksig_oracle as O
+  return O.signature_kernel(X, Y, n_levels=N_LEVELS, order=ORDER,
+                            normalize=True, param=BANDWIDTH)
+
+
+def cpu_sample(nx, ny, seed, pool=None):
+  """Times the oracle on an nx x ny block (plus its diagonal passes)."""
+  X = make_walks(nx, SEQ_LEN, D_WALK, seed).astype(np.float64)
+  Y = make_walks(ny, SEQ_LEN, D_WALK, seed + 1).astype(np.float64)
+  t0 = time.perf_counter()
+  if pool is None:
+    _cpu_chunk((X, Y))
+  else:
+    rows = np.array_split(np.arange(nx), len(pool._pool))
+    list(pool.map(_cpu_chunk, [(X[r], Y) for r in rows if len(r)]))
+  return time.perf_counter() - t0
+
+
+# ---------------------------------------------------------------------------
+# Clock sampling during the timed region.
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+  FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+            'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+            'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+  def __init__(self, gpu_index):
+    self.idx = gpu_index
+    self.proc = None
+    self.path = None
+
+  def start(self):
+    try:
+      out_dir = os.path.join(ROOT, 'gpurun_out')
+      os.makedirs(out_dir, exist_ok=True)
+      self.path = os.path.join(out_dir, f'clocks_gpu{self.idx}.csv')
+      self.f = open(self.path, 'w')
+      self.proc = subprocess.Popen(
+          ['nvidia-smi', f'--id={self.idx}', f'--query-gpu={self.FIELDS}',
+           '--format=csv,noheader,nounits', '-lms', '100'],
+          stdout=self.f, stderr=subprocess.DEVNULL)
+    except Exception:  # noqa: BLE001 - clocks are best effort
+      self.proc = None
+
+  def stop(self):
+    if self.proc is None:
+      return None
+    self.proc.terminate()
+    try:
+      self.proc.wait(timeout=5)
+    except Exception:  # noqa: BLE001
+      self.proc.kill()
+    self.f.close()
+    sm, mx, reasons = [], None, set()
+    names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown',
+             'sw_power_cap']
+    with open(self.path) as f:
+      for line in f:
+        parts = [p.strip() for p in line.split(',')]
+        if len(parts) < 9:
+          continue
+        try:
+          sm.append(float(parts[1]))
+          mx = float(parts[2])
+        except ValueError:
+          continue
+        for n, v in zip(names, parts[5:9]):
+          if v.lower() == 'active':
+            reasons.add(n)
+    if not sm:
+      return None
+    return {'sm_mhz': statistics.median(sm), 'sm_max_mhz': mx,
+            'reasons': sorted(reasons), 'samples': len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# GPU arm.
+# ---------------------------------------------------------------------------
+
+def run_ours(args, rank, world, dist):
+  import torch
+
+  import ksig_b200 as K
+  from ksig_b200 import _engine as E
+  from ksig_b200 import _lib as Lb
+
+  dev = torch.device('cuda', torch.cuda.current_device())
+  X = make_walks(N_SEQ, SEQ_LEN, D_WALK, 2 + 2 * rank)
+  Y = make_walks(N_SEQ, SEQ_LEN, D_WALK, 3 + 2 * rank)
+  Xd = torch.as_tensor(X, device=dev)
+  Yd = torch.as_tensor(Y, device=dev)
+  kern = K.SignatureKernel(n_levels=N_LEVELS, order=ORDER, normalize=True,
+                           static_kernel=K.RBFKernel(BANDWIDTH))
+  lib = Lb.lib()
+  flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+
+  def step():
+    return kern(Xd, Yd, return_on_gpu=True)
+
+  def barrier():
+    if dist is not None:
+      dist.barrier()
+    torch.cuda.synchronize()
+
+  for _ in range(args.warmup):
+    step()
+  barrier()
+  stream = torch.cuda.current_stream()
+  evs = [(torch.cuda.Event(enable_timing=True),
+          torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+  clocks = ClockSampler(dev.index if dev.index is not None else 0)
+  clocks.start()
+  launches0 = lib.ksig_launch_count()
+  barrier()
+  for i in range(args.steps):
+    flush.fill_(i & 0xff)  # evict L2 (126 MB) between steps, untimed
+    evs[i][0].record(stream)
+    step()
+    evs[i][1].record(stream)
+  barrier()
+  launches = lib.ksig_launch_count() - launches0
+  clk = clocks.stop()
+  ms = [a.elapsed_time(b) for a, b in evs]
+  t_step = sum(ms) / len(ms)
+  if dist is not None:
+    t = torch.tensor([t_step], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    t_step = float(t.item())
+
+  # Dominant kernel: the 512 x 512 pair sweep, timed alone with CUDA events
+  # recorded by the library on its launch stream.
+  Xs, Ys = E.Seqs(Xd), E.Seqs(Yd)
+  lib.ksig_profile_read(None, None)
+  lib.ksig_profile_enable(1)
+  nrep = 5
+  for _ in range(nrep):
+    flush.fill_(1)
+    E.sig_levels(Xs, Ys, Lb.PAIRS_FULL, N_LEVELS, ORDER, True, Lb.STATIC_RBF,
+                 BANDWIDTH)
+  torch.cuda.synchronize()
+  lib.ksig_profile_enable(0)
+  tot = ctypes.c_double(0)
+  cnt = ctypes.c_longlong(0)
+  lib.ksig_profile_read(ctypes.byref(tot), ctypes.byref(cnt))
+  k_ms = tot.value / max(cnt.value, 1)
+  peak = ctypes.c_double(0)
+  Lb.check(lib.ksig_fp32_peak(ctypes.byref(peak),
+                              ctypes.c_void_p(stream.cuda_stream)))
+  d = D_WALK + 1
+  G = SEQ_LEN * SEQ_LEN
+  cells = (SEQ_LEN - 1) ** 2
+  flops_pair = G * (2 * d + 4) + cells * (4 + 4 * (N_LEVELS - 1))
+  achieved = flops_pair * N_SEQ * N_SEQ / (k_ms * 1e-3) / 1e12
+  traffic = None
+  tpath = os.path.join(ROOT, 'profiles', 'dp_fwd_traffic.json')
+  if os.path.exists(tpath):
+    with open(tpath) as f:
+      traffic = json.load(f).get('bytes_per_launch')
+
+  # End to end through the public API from pinned host memory.
+  Xh = torch.as_tensor(X).pin_memory()
+  Yh = torch.as_tensor(Y).pin_memory()
+  for _ in range(2):
+    kern(Xh, Yh)
+  barrier()
+  e_ms = []
+  for i in range(args.steps):
+    flush.fill_(i & 0xff)
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    Kh = kern(Xh, Yh)  # H2D of X, Y; D2H of the [512, 512] result
+    b.record(stream)
+    b.synchronize()
+    e_ms.append(a.elapsed_time(b))
+  e_step = sum(e_ms) / len(e_ms)
+  if dist is not None:
+    t = torch.tensor([e_step], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e_step = float(t.item())
+  assert Kh.shape == (N_SEQ, N_SEQ)
+
+  cpu = None
+  if rank == 0 and world == 1 and not args.no_cpu:
+    n = args.cpu_pairs
+    secs = cpu_sample(n, n, 100)
+    cpu = {'value': n * n / secs, 'unit': UNIT, 'cores': 1, 'kind': 'port',
+           'sample': f'{n}x{n} pairs of the same workload (+ diagonal passes),'
+                     ' NumPy FP64 restatement of the reference recursion '
+                     '(oracle/ksig_oracle.py), single process',
+           'seconds': secs}
+
+  entries = N_SEQ * N_SEQ * world
+  if rank == 0:
+    line = {
+        'metric': METRIC, 'value': entries / (t_step * 1e-3), 'unit': UNIT,
+        'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
+        'ms_per_step': t_step, 'higher_is_better': True, 'scaling': 'weak',
+        'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+        'config': config(world, {'l2': 'flushed (256 MB write) between steps'}),
+        'roofline': {'bound': 'fp32', 'achieved': achieved,
+                     'peak': peak.value, 'unit': 'TFLOP/s',
+                     'frac': achieved / peak.value if peak.value else None,
+                     'traffic': traffic,
+                     'kernel': 'dp_fwd_kernel (512x512 pair sweep)',
+                     'kernel_ms': k_ms,
+                     'peak_source': 'measured live: FP32 FMA-chain probe '
+                                    '(ksig_fp32_peak) on this GPU'},
+        'e2e': {'value': entries / (e_step * 1e-3), 'unit': UNIT,
+                'ms_per_step': e_step,
+                'h2d_bytes_per_step': int(X.nbytes + Y.nbytes),
+                'd2h_bytes_per_step': int(N_SEQ * N_SEQ * 4)},
+        'gpu_launches': int(launches),
+        'clocks': clk,
+        'cpu_baseline': cpu,
+    }
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# Reference arm: the reference recursion on the host cores.
+# ---------------------------------------------------------------------------
+
+def run_reference(args, rank, world):
+  if rank != 0:
+    return
+  import multiprocessing as mp
+  cores = os.cpu_count() or 1
+  ctx = mp.get_context('spawn')
+  n = args.ref_pairs
+  with ctx.Pool(cores) as pool:
+    for _ in range(args.warmup):
+      cpu_sample(n, n, 7, pool)
+    t = [cpu_sample(n, n, 7 + i, pool) for i in range(args.steps)]
+  secs = sum(t) / len(t)
+  value = n * n / secs
+  line = {
+      'metric': METRIC, 'value': value, 'unit': UNIT, 'impl': 'reference',
+      'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
+      'ms_per_step': secs * 1e3, 'higher_is_better': True, 'scaling': 'weak',
+      'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+      'config': config(world),
+      'cpu_baseline': {'value': value, 'unit': UNIT, 'cores': cores,
+                       'kind': 'port',
+                       'sample': f'{n}x{n} pairs per step (+ diagonal passes) '
+                                 'of the same workload; the reference needs '
+                                 'CuPy on a GPU, so its recursion runs as the '
+                                 'NumPy restatement in oracle/ over a '
+                                 f'{cores}-process pool'},
+      'e2e': {'value': value, 'unit': UNIT, 'h2d_bytes_per_step': 0,
+              'd2h_bytes_per_step': 0},
+  }
+  print(json.dumps(line))
+
+
+def main():
+  ap = argparse.ArgumentParser()
+  ap.add_argument('--gpus', type=int, default=1)
+  ap.add_argument('--steps', type=int, default=20)
+  ap.add_argument('--warmup', type=int, default=5)
+  ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+  ap.add_argument('--cpu-pairs', type=int, default=40)
+  ap.add_argument('--ref-pairs', type=int, default=32)
+  ap.add_argument('--no-cpu', action='store_true')
+  args = ap.parse_args()
+  args.warmup = max(args.warmup, 3)
+  world = int(os.environ.get('WORLD_SIZE', '1'))
+  rank = int(os.environ.get('RANK', '0'))
+  if args.impl == 'reference':
+    run_reference(args, rank, world)
+    return
+  import torch
+  dist = None
+  if world > 1:
+    import datetime
+    import torch.distributed as tdist
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    torch.cuda.set_device(local)
+    tdist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
+    dist = tdist
+  else:
+    torch.cuda.set_device(0)
+  try:
+    run_ours(args, rank, world, dist)
+  finally:
+    if dist is not None:
+      dist.barrier()
+      dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+  main()

@@ -1,0 +1,178 @@
+/*
+ * ksig_b200 — C ABI of the B200 (sm_100a) signature-kernel library.
+ *
+ * Every entry point takes caller-owned DEVICE pointers, a caller-owned
+ * device workspace, and a cudaStream_t passed as `void*` (NULL = legacy
+ * default stream).  Calls are asynchronous on that stream except where a
+ * function says otherwise; they return a KSIG_* status code and never
+ * allocate device memory.  Sequences are dense row-major arrays
+ * [n, L, d] of float32 or float64 (dtype KSIG_DTYPE_*); an optional int32
+ * device array `len[n]` gives each sequence's true number of points
+ * (2..L; points past it are ignored, which is exactly the reference's
+ * behaviour on edge-padded arrays).  The arithmetic runs in the input
+ * dtype (float32 inputs: FP32 with FP64 level/normalisation reductions;
+ * float64 inputs: FP64 throughout).
+ *
+ * Reference interfaces replaced (tgcsaba/KSig 1.0.0, paths within the
+ * project):
+ *   ksig_signature_kern      SignatureKernel._compute_kernel
+ *                            (ksig/kernels.py:147-164) = _compute_embedding
+ *                            (ksig/kernels.py:124-145, static Gram through
+ *                            RBFKernel._K ksig/static/kernels.py:248-260 or
+ *                            LinearKernel._K :145-155) followed by
+ *                            signature_kern(..., return_levels=True)
+ *                            (ksig/algorithms.py:22-140).
+ *   ksig_signature_kern_pde  SignaturePDEKernel._compute_kernel
+ *                            (ksig/kernels.py:242-256) = static Gram +
+ *                            signature_kern_pde (ksig/algorithms.py:402-446)
+ *                            and its Numba kernel (:344-399).
+ *   ksig_normalize_levels    the normalisation and level mean of
+ *                            SignatureKernel._K (ksig/kernels.py:190-214),
+ *                            robust_sqrt (ksig/utils.py:173-182).
+ *   ksig_*_bwd               no reference counterpart (the reference has no
+ *                            gradients); adjoints of the two kernels above.
+ */
+#ifndef KSIG_B200_H_
+#define KSIG_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define KSIG_OK 0
+#define KSIG_ERR_INVALID 1     /* invalid argument (shape, parameter, dtype) */
+#define KSIG_ERR_UNSUPPORTED 2 /* no compiled kernel for this configuration  */
+#define KSIG_ERR_WORKSPACE 3   /* workspace smaller than required            */
+#define KSIG_ERR_CUDA 4        /* CUDA runtime error (see ksig_last_error)   */
+#define KSIG_ERR_DEVICE 5      /* device-side check failed (bounded wait,
+                                  bounds check); the context stays usable    */
+
+/* Static (state-space) kernels. */
+#define KSIG_STATIC_RBF 0    /* exp(-|x-y|^2 / max(2 param^2, 1e-12))  */
+#define KSIG_STATIC_LINEAR 1 /* param * <x, y>                          */
+
+/* Element types. */
+#define KSIG_DTYPE_F32 0
+#define KSIG_DTYPE_F64 1
+
+/* Which (row, column) sequence pairs a call evaluates; output entry p of a
+ * per-pair array belongs to pair p of this enumeration. */
+#define KSIG_PAIRS_FULL 0  /* all nX*nY pairs, p = a*nY + b                  */
+#define KSIG_PAIRS_UPPER 1 /* X against itself, a <= b, row-major triangle;
+                              p = a*nX - a*(a-1)/2 + (b-a); Y is ignored      */
+#define KSIG_PAIRS_DIAG 2  /* (a, a) for a < nX; Y is ignored                 */
+#define KSIG_PAIRS_LIST 3  /* explicit int32 pairs (a, b), pair_list[2p..2p+1]*/
+
+/* Library version string. */
+const char* ksig_version(void);
+
+/* Copies the message of the last failing call on this host thread into buf
+ * (NUL-terminated, truncated to n bytes); returns its full length. */
+size_t ksig_last_error(char* buf, size_t n);
+
+/* Number of pairs a pairs_mode enumerates. */
+long long ksig_num_pairs(int pairs_mode, int nX, int nY, int n_list);
+
+/* Workspace (bytes) required by ksig_signature_kern with these sizes. */
+size_t ksig_signature_kern_workspace(int nX, int LX, int nY, int LY, int d,
+                                     int dtype, int n_levels, int order,
+                                     int difference, int pairs_mode,
+                                     int n_list);
+
+/*
+ * Truncated signature kernel per level (replaces
+ * SignatureKernel._compute_kernel with return_levels=True,
+ * ksig/kernels.py:147-164 and ksig/algorithms.py:22-140).
+ *
+ *   out_levels  float64 [n_levels + 1, P] with P = ksig_num_pairs(...);
+ *               row 0 is 1 (level 0), row k the level-k kernel.
+ *   order       Alg. 3 when the clamped order is 1, Alg. 6 otherwise; the
+ *               clamp is that of ksig/algorithms.py:37 (order <= 0 or
+ *               order >= n_levels -> n_levels).
+ *   difference  1: increments of the lifted paths (second difference of the
+ *               static Gram, ksig/algorithms.py:63-64); 0: the Gram itself.
+ */
+int ksig_signature_kern(const void* X, const int32_t* lenX, int nX, int LX,
+                        const void* Y, const int32_t* lenY, int nY, int LY,
+                        int d, int dtype, int static_kind,
+                        double static_param, int n_levels, int order,
+                        int difference, int pairs_mode,
+                        const int32_t* pair_list, int n_list,
+                        double* out_levels, void* workspace,
+                        size_t workspace_bytes, void* stream);
+
+/* Workspace (bytes) required by ksig_signature_kern_pde. */
+size_t ksig_signature_kern_pde_workspace(int nX, int LX, int nY, int LY,
+                                         int d, int dtype, int dyadic_order,
+                                         int difference, int pairs_mode,
+                                         int n_list);
+
+/*
+ * Signature-PDE kernel (replaces SignaturePDEKernel._compute_kernel,
+ * ksig/kernels.py:242-256, and signature_kern_pde,
+ * ksig/algorithms.py:402-446).  Second-order Goursat scheme of
+ * ksig/algorithms.py:384-385 with boundary value 1.  dyadic_order k > 0
+ * refines every cell into 2^k x 2^k cells with increment q / 4^k (no
+ * reference counterpart; k = 0 is the reference scheme).
+ *   out  float64 [P].
+ */
+int ksig_signature_kern_pde(const void* X, const int32_t* lenX, int nX,
+                            int LX, const void* Y, const int32_t* lenY,
+                            int nY, int LY, int d, int dtype,
+                            int static_kind, double static_param,
+                            int dyadic_order, int difference, int pairs_mode,
+                            const int32_t* pair_list, int n_list,
+                            double* out, void* workspace,
+                            size_t workspace_bytes, void* stream);
+
+/*
+ * Normalisation and level mean (replaces ksig/kernels.py:190-214).
+ *   levels   float64 [n_lev, P] from one of the calls above with pairs_mode
+ *            FULL (P = nX*nY) or UPPER (P = nX(nX+1)/2, result mirrored).
+ *   diagX    float64 [n_lev, nX] per-level K(x_a, x_a) (DIAG call), or NULL
+ *            to take the diagonal of `levels` (UPPER, or FULL with X = Y).
+ *   diagY    float64 [n_lev, nY], or NULL to reuse diagX.
+ *   normalize 1: K_l / (max(sqrt(max(Kx_l, 1e-12)), 1e-12) *
+ *            max(sqrt(max(Ky_l, 1e-12)), 1e-12)) then the mean over the
+ *            n_lev levels; 0: the sum over levels.
+ *   out      [nX, nY] of out_dtype (KSIG_DTYPE_*).
+ */
+int ksig_normalize_levels(const double* levels, int n_lev, int pairs_mode,
+                          int nX, int nY, const double* diagX,
+                          const double* diagY, int normalize, void* out,
+                          int out_dtype, void* stream);
+
+/*
+ * Synchronises `stream`, then reads and clears the device status word that
+ * the kernels of the last call on `workspace` wrote (lengths outside [1, L]
+ * are clamped and flagged there).  Returns KSIG_OK, KSIG_ERR_INVALID or
+ * KSIG_ERR_DEVICE.  No reference counterpart (CuPy raises on the host).
+ */
+int ksig_workspace_status(void* workspace, void* stream);
+
+/*
+ * Measurement helpers (no reference counterpart).
+ *   ksig_launch_count    kernels launched by this library since it was loaded.
+ *   ksig_profile_enable  when on, every main sweep kernel is bracketed by CUDA
+ *                        events on its own stream.
+ *   ksig_profile_read    waits for the recorded events and returns the summed
+ *                        kernel time (ms) and the number of timed launches
+ *                        since the last read.
+ *   ksig_fp32_peak       measures this GPU's FP32 FMA throughput (TFLOP/s,
+ *                        2 flops per FMA) with an FMA-chain kernel on `stream`
+ *                        (synchronous).
+ */
+unsigned long long ksig_launch_count(void);
+void ksig_profile_enable(int on);
+int ksig_profile_read(double* total_ms, long long* launches);
+int ksig_fp32_peak(double* tflops, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KSIG_B200_H_ */

@@ -1,0 +1,13 @@
+"""ksig_b200: B200 (sm_100a) signature kernels with KSig's callable API.
+
+Importing the package does not touch the GPU; the CUDA library
+(``lib/libksig_b200.so``) is loaded on first use.
+"""
+
+from . import kernels  # noqa: F401
+from . import static  # noqa: F401
+from . import utils  # noqa: F401
+from .kernels import SignatureKernel, SignaturePDEKernel  # noqa: F401
+from .static.kernels import LinearKernel, RBFKernel  # noqa: F401
+
+__version__ = '0.1.0'

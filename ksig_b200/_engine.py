@@ -1,0 +1,131 @@
+"""Device-side calls into the C ABI on PyTorch CUDA tensors.
+
+PyTorch only provides device memory and the current stream here; every
+arithmetic step runs in ``libksig_b200.so``.
+"""
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+
+def _ptr(t):
+  return ctypes.c_void_p(0 if t is None else t.data_ptr())
+
+
+def _stream():
+  return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _dtype_code(t):
+  if t.dtype == torch.float64:
+    return L.DTYPE_F64
+  if t.dtype == torch.float32:
+    return L.DTYPE_F32
+  raise ValueError(f'unsupported dtype {t.dtype}; expected float32/float64')
+
+
+def _workspace(nbytes, device):
+  return torch.empty(max(int(nbytes), 16), dtype=torch.uint8, device=device)
+
+
+class Seqs:
+  """A batch of sequences on the device: dense ``[n, L, d]`` plus lengths."""
+
+  __slots__ = ('data', 'lengths', 'n', 'L', 'd')
+
+  def __init__(self, data, lengths=None):
+    if not data.is_cuda:
+      raise ValueError('sequences must live on a CUDA device')
+    self.data = data.contiguous()
+    self.n, self.L, self.d = self.data.shape
+    if lengths is not None:
+      lengths = lengths.to(device=data.device, dtype=torch.int32).contiguous()
+    self.lengths = lengths
+
+
+def num_pairs(mode, nX, nY, n_list=0):
+  return int(L.lib().ksig_num_pairs(mode, nX, nY, n_list))
+
+
+def sig_levels(X, Y, mode, n_levels, order, difference, kind, param,
+               pair_list=None):
+  """Per-level signature kernels ``[n_levels+1, P]`` (float64)."""
+  lib = L.lib()
+  Yv = X if Y is None else Y
+  dt = _dtype_code(X.data)
+  if Y is not None and Y.data.dtype != X.data.dtype:
+    raise ValueError('X and Y must share a dtype')
+  if Y is not None and Y.d != X.d:
+    raise ValueError('X and Y must have the same number of features')
+  n_list = 0 if pair_list is None else pair_list.shape[0]
+  P = num_pairs(mode, X.n, Yv.n, n_list)
+  out = torch.empty((n_levels + 1, max(P, 0)), dtype=torch.float64,
+                    device=X.data.device)
+  ws_bytes = lib.ksig_signature_kern_workspace(
+      X.n, X.L, Yv.n, Yv.L, X.d, dt, n_levels, order, int(difference), mode,
+      n_list)
+  if ws_bytes == 0:
+    L.check(L.ERR_UNSUPPORTED if 'no compiled' in L.last_error()
+            else L.ERR_INVALID)
+  ws = _workspace(ws_bytes, X.data.device)
+  rc = lib.ksig_signature_kern(
+      _ptr(X.data), _ptr(X.lengths), X.n, X.L, _ptr(Yv.data),
+      _ptr(Yv.lengths), Yv.n, Yv.L, X.d, dt, kind, float(param), n_levels,
+      order, int(difference), mode, _ptr(pair_list), n_list, _ptr(out),
+      _ptr(ws), ws_bytes, _stream())
+  L.check(rc)
+  return out
+
+
+def pde_values(X, Y, mode, dyadic_order, difference, kind, param,
+               pair_list=None):
+  """Signature-PDE kernel per pair ``[P]`` (float64)."""
+  lib = L.lib()
+  Yv = X if Y is None else Y
+  dt = _dtype_code(X.data)
+  if Y is not None and Y.data.dtype != X.data.dtype:
+    raise ValueError('X and Y must share a dtype')
+  if Y is not None and Y.d != X.d:
+    raise ValueError('X and Y must have the same number of features')
+  n_list = 0 if pair_list is None else pair_list.shape[0]
+  P = num_pairs(mode, X.n, Yv.n, n_list)
+  out = torch.empty((max(P, 0),), dtype=torch.float64, device=X.data.device)
+  ws_bytes = lib.ksig_signature_kern_pde_workspace(
+      X.n, X.L, Yv.n, Yv.L, X.d, dt, dyadic_order, int(difference), mode,
+      n_list)
+  if ws_bytes == 0:
+    L.check(L.ERR_UNSUPPORTED if 'no compiled' in L.last_error()
+            else L.ERR_INVALID)
+  ws = _workspace(ws_bytes, X.data.device)
+  rc = lib.ksig_signature_kern_pde(
+      _ptr(X.data), _ptr(X.lengths), X.n, X.L, _ptr(Yv.data),
+      _ptr(Yv.lengths), Yv.n, Yv.L, X.d, dt, kind, float(param),
+      dyadic_order, int(difference), mode, _ptr(pair_list), n_list,
+      _ptr(out), _ptr(ws), ws_bytes, _stream())
+  L.check(rc)
+  return out
+
+
+def normalize_levels(levels, mode, nX, nY, diagX, diagY, normalize,
+                     out_dtype):
+  """Normalisation / level mean (or level sum) -> ``[nX, nY]``."""
+  n_lev = levels.shape[0]
+  out = torch.empty((nX, nY), dtype=out_dtype, device=levels.device)
+  code = L.DTYPE_F64 if out_dtype == torch.float64 else L.DTYPE_F32
+  rc = L.lib().ksig_normalize_levels(
+      _ptr(levels), n_lev, mode, nX, nY, _ptr(diagX), _ptr(diagY),
+      int(normalize), _ptr(out), code, _stream())
+  L.check(rc)
+  return out
+
+
+def to_numpy(t):
+  return t.detach().cpu().numpy()
+
+
+def np_dtype(t):
+  return np.float64 if t.dtype == torch.float64 else np.float32

@@ -1,0 +1,206 @@
+"""Builds ``ksig_b200/lib/libksig_b200.so`` (sm_100a) in-tree with nvcc.
+
+The hot kernels are templates over the compute type, the padded point
+dimension KD, the columns per lane C, the number of levels NL and the order
+P (or the dyadic refinement F for the PDE).  This script writes one
+translation unit per group of instantiations under ``csrc/gen/`` together
+with a registry table the C ABI searches at run time, compiles the units in
+parallel and links the shared library.  Rebuilds are incremental (object
+files newer than every source they depend on are kept).
+
+    python -m ksig_b200.build [-j N] [--force]
+"""
+
+import argparse
+import concurrent.futures as cf
+import itertools
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, 'csrc')
+GEN = os.path.join(CSRC, 'gen')
+OBJ = os.path.join(HERE, '_build')
+LIB_DIR = os.path.join(HERE, 'lib')
+LIB = os.path.join(LIB_DIR, 'libksig_b200.so')
+
+ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
+NVCC_FLAGS = ['-O3', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC',
+              '-Xcompiler', '-O2', '--expt-relaxed-constexpr', '-ftz=true']
+WPB = 4  # warps per block of the sweep kernels
+
+KD_ALL = [2, 4, 6, 8, 10, 12, 16, 24, 32]
+KD_FEW = [4, 8, 16, 32]
+NL_ALL = [1, 2, 3, 4, 5, 6, 8]
+
+
+def instances():
+  """(op, dtype, kd, c, nl, p, diff) tuples.  op: dp/pde/dpb/pdeb."""
+  out = []
+  add = out.append
+  # DP forward, float.
+  for nl, kd, c in itertools.product(NL_ALL, KD_ALL, [2, 4, 7]):
+    add(('dp', 'f32', kd, c, nl, 1, 1))
+  for nl, kd, c in itertools.product([2, 3, 4, 5, 6, 8], KD_ALL, [2, 4]):
+    add(('dp', 'f32', kd, c, nl, 2, 1))
+  for p, nls in ((3, [3, 4, 5, 6, 8]), (4, [4, 5, 6, 8])):
+    for nl, kd in itertools.product(nls, KD_FEW):
+      add(('dp', 'f32', kd, 2, nl, p, 1))
+  for p, nls in ((1, NL_ALL), (2, [2, 3, 4, 5, 6, 8])):
+    for nl, kd in itertools.product(nls, KD_FEW):
+      add(('dp', 'f32', kd, 2, nl, p, 0))
+  # DP forward, double.
+  for p, nls, kds in ((1, NL_ALL, KD_ALL), (2, [2, 3, 4, 5, 6, 8], KD_ALL),
+                      (3, [3, 4, 5, 6, 8], KD_FEW), (4, [4, 5, 6, 8], KD_FEW)):
+    for nl, kd in itertools.product(nls, kds):
+      add(('dp', 'f64', kd, 2, nl, p, 1))
+  for p, nls in ((1, NL_ALL), (2, [2, 3, 4, 5, 6, 8])):
+    for nl, kd in itertools.product(nls, KD_FEW):
+      add(('dp', 'f64', kd, 2, nl, p, 0))
+  # PDE forward.
+  for f, kd, c in itertools.product([1, 2, 4, 8], KD_ALL, [2, 4, 8]):
+    add(('pde', 'f32', kd, c, 0, f, 1))
+  for f, kd in itertools.product([1, 2, 4, 8], KD_ALL):
+    add(('pde', 'f64', kd, 2, 0, f, 1))
+  for dt in ('f32', 'f64'):
+    for f, kd in itertools.product([1, 2, 4], KD_FEW):
+      add(('pde', dt, kd, 2, 0, f, 0))
+  return out
+
+
+OPS = {
+    'dp': ('OP_DP_FWD', 'dp_fwd_kernel<{T}, {kd}, {c}, {nl}, {p}, {diff}, {wpb}>'),
+    'pde': ('OP_PDE_FWD', 'pde_fwd_kernel<{T}, {kd}, {c}, {p}, {diff}, {wpb}>'),
+}
+
+
+def _group_key(inst):
+  op, dt, kd, c, nl, p, diff = inst
+  return f'{op}_{dt}_p{p}_d{diff}_kd{kd}'
+
+
+def generate():
+  """Writes csrc/gen/*.cu; returns the list of generated unit paths."""
+  os.makedirs(GEN, exist_ok=True)
+  groups = {}
+  for inst in instances():
+    groups.setdefault(_group_key(inst), []).append(inst)
+  units = []
+  tables = []
+  for key, insts in sorted(groups.items()):
+    lines = ['// Generated by ksig_b200/build.py; do not edit.',
+             '#include "../sweep.cuh"', '#include "../registry.h"',
+             'namespace ksig {']
+    ents = []
+    for op, dt, kd, c, nl, p, diff in insts:
+      T = 'float' if dt == 'f32' else 'double'
+      opname, tmpl = OPS[op]
+      name = tmpl.format(T=T, kd=kd, c=c, nl=nl, p=p,
+                         diff='true' if diff else 'false', wpb=WPB)
+      ents.append(f'  {{{opname}, {int(dt == "f64")}, {kd}, {c}, {nl}, {p}, '
+                  f'{diff}, {WPB}, (const void*)&{name}}},')
+    lines.append(f'extern const KernelEntry kTab_{key}[] = {{')
+    lines += ents
+    lines.append('};')
+    lines.append(f'extern const int kTabN_{key} = {len(ents)};')
+    lines.append('}  // namespace ksig')
+    path = os.path.join(GEN, f'inst_{key}.cu')
+    _write_if_changed(path, '\n'.join(lines) + '\n')
+    units.append(path)
+    tables.append(key)
+  reg = ['// Generated by ksig_b200/build.py; do not edit.',
+         '#include "../registry.h"', 'namespace ksig {']
+  for key in tables:
+    reg.append(f'extern const KernelEntry kTab_{key}[];')
+    reg.append(f'extern const int kTabN_{key};')
+  reg.append('const KernelTable kAllTables[] = {')
+  for key in tables:
+    reg.append(f'  {{kTab_{key}, {len(groups[key])}}},')
+  reg.append('};')
+  reg.append(f'const int kNumTables = {len(tables)};')
+  reg.append('}  // namespace ksig')
+  path = os.path.join(GEN, 'registry_tables.cu')
+  _write_if_changed(path, '\n'.join(reg) + '\n')
+  units.append(path)
+  return units
+
+
+def _write_if_changed(path, text):
+  if os.path.exists(path):
+    with open(path) as f:
+      if f.read() == text:
+        return
+  with open(path, 'w') as f:
+    f.write(text)
+
+
+def _headers():
+  hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC)
+        if f.endswith(('.cuh', '.h'))]
+  hs.append(os.path.join(ROOT, 'include', 'ksig_b200.h'))
+  return hs
+
+
+def _nvcc():
+  cand = shutil.which('nvcc') or '/usr/local/cuda/bin/nvcc'
+  return cand
+
+
+def _compile(src, obj, force):
+  deps = [src] + _headers() + [os.path.abspath(__file__)]
+  if (not force and os.path.exists(obj)
+      and os.path.getmtime(obj) >= max(os.path.getmtime(d) for d in deps)):
+    return obj, None
+  cmd = [_nvcc()] + ARCH + NVCC_FLAGS + ['-I', os.path.join(ROOT, 'include'),
+                                         '-c', src, '-o', obj]
+  r = subprocess.run(cmd, capture_output=True, text=True)
+  if r.returncode != 0:
+    return obj, f'{" ".join(cmd)}\n{r.stdout}\n{r.stderr}'
+  return obj, None
+
+
+def build(jobs=None, force=False, verbose=True):
+  units = generate()
+  units = [os.path.join(CSRC, 'capi.cu')] + units
+  os.makedirs(OBJ, exist_ok=True)
+  os.makedirs(LIB_DIR, exist_ok=True)
+  objs = []
+  jobs = jobs or os.cpu_count() or 4
+  errors = []
+  with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
+    futs = []
+    for u in units:
+      obj = os.path.join(OBJ, os.path.basename(u)[:-3] + '.o')
+      objs.append(obj)
+      futs.append(ex.submit(_compile, u, obj, force))
+    for f in futs:
+      _, err = f.result()
+      if err:
+        errors.append(err)
+  if errors:
+    raise RuntimeError('nvcc failed:\n' + '\n'.join(errors[:3]))
+  if (force or not os.path.exists(LIB)
+      or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs)):
+    cmd = [_nvcc()] + ARCH + ['-shared', '-o', LIB] + objs + ['-lcudart']
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+      raise RuntimeError(f'link failed: {r.stdout}\n{r.stderr}')
+  if verbose:
+    print(f'built {LIB} ({len(instances())} kernel instantiations, '
+          f'{len(units)} units)')
+  return LIB
+
+
+def main():
+  ap = argparse.ArgumentParser()
+  ap.add_argument('-j', type=int, default=None)
+  ap.add_argument('--force', action='store_true')
+  a = ap.parse_args()
+  build(jobs=a.j, force=a.force)
+
+
+if __name__ == '__main__':
+  sys.exit(main())

@@ -1,0 +1,518 @@
+// C ABI of the ksig_b200 library: argument checks, workspace layout, packing
+// and kernel dispatch.  Declarations and reference citations live in
+// include/ksig_b200.h.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <atomic>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "normalize.cuh"
+#include "pack.cuh"
+#include "registry.h"
+#include "sweep.cuh"
+
+namespace ksig {
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  return fail(KSIG_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define KSIG_CUDA(call)                                   \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);   \
+  } while (0)
+
+std::atomic<unsigned long long> g_launches{0};
+
+// Optional CUDA-event timing of the main sweep kernels (bench / profiling).
+struct Profiler {
+  std::mutex mu;
+  bool on = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pool;
+};
+Profiler& prof() {
+  static Profiler p;
+  return p;
+}
+
+// Launches `func` and, when profiling is on, brackets it with CUDA events on
+// the same stream.
+cudaError_t launch_main(const void* func, dim3 grid, dim3 block, void** args, cudaStream_t st) {
+  Profiler& P = prof();
+  std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
+  bool timed = false;
+  {
+    std::lock_guard<std::mutex> lk(P.mu);
+    if (P.on) {
+      if (!P.pool.empty()) {
+        ev = P.pool.back();
+        P.pool.pop_back();
+      } else {
+        cudaEventCreate(&ev.first);
+        cudaEventCreate(&ev.second);
+      }
+      timed = ev.first && ev.second;
+    }
+  }
+  if (timed) cudaEventRecord(ev.first, st);
+  cudaError_t e = cudaLaunchKernel(func, grid, block, args, 0, st);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (timed) {
+    cudaEventRecord(ev.second, st);
+    std::lock_guard<std::mutex> lk(P.mu);
+    P.pending.push_back(ev);
+  }
+  return e;
+}
+
+int sm_count() {
+  static std::mutex mu;
+  static std::vector<int> cache;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  std::lock_guard<std::mutex> lk(mu);
+  if ((int)cache.size() <= dev) cache.resize(dev + 1, 0);
+  if (cache[dev] == 0) {
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    cache[dev] = n;
+  }
+  return cache[dev];
+}
+
+// Finds the best compiled instantiation: exact op/dtype/order/diff, the
+// smallest kd >= need_kd, the smallest nl >= need_nl (DP: extra levels are
+// computed and dropped), and the column count closest to want_c (prefer the
+// largest c <= want_c, else the smallest above).
+const KernelEntry* find_kernel(int op, int f64, int need_kd, int want_c, int need_nl,
+                               int p, int diff) {
+  const KernelEntry* best = nullptr;
+  auto better = [&](const KernelEntry& e) {
+    if (!best) return true;
+    if (e.kd != best->kd) return e.kd < best->kd;
+    if (e.nl != best->nl) return e.nl < best->nl;
+    const bool eb = e.c <= want_c, bb = best->c <= want_c;
+    if (eb != bb) return eb;
+    return eb ? e.c > best->c : e.c < best->c;
+  };
+  for (int t = 0; t < kNumTables; ++t) {
+    for (int i = 0; i < kAllTables[t].n; ++i) {
+      const KernelEntry& e = kAllTables[t].entries[i];
+      if (e.op != op || e.f64 != f64 || e.p != p || e.diff != diff) continue;
+      if (e.kd < need_kd || e.nl < need_nl) continue;
+      if (better(e)) best = &e;
+    }
+  }
+  return best;
+}
+
+size_t align_up(size_t v, size_t a = 256) { return (v + a - 1) / a * a; }
+
+// Workspace carve-up shared by the forward kernels.
+struct FwdPlan {
+  int f64, kd, rs, c, nl, nl_out, p, diff, nx_exchange;
+  long long ntasks;
+  int multi, grid, wpb;
+  long long rows_max, scratch_per_warp;
+  size_t off_status, off_xr, off_yr, off_xstart, off_ystart, off_xlen, off_ylen,
+      off_scratch, total;
+  const KernelEntry* k;
+};
+
+long long num_pairs(int mode, int nX, int nY, int n_list) {
+  switch (mode) {
+    case KSIG_PAIRS_FULL: return (long long)nX * nY;
+    case KSIG_PAIRS_UPPER: return (long long)nX * (nX + 1) / 2;
+    case KSIG_PAIRS_DIAG: return nX;
+    case KSIG_PAIRS_LIST: return n_list;
+  }
+  return -1;
+}
+
+// Column count per lane: smallest c whose strip covers the longest column
+// sequence in one strip, capped by what the register budget allows.
+int want_cols(int ly_cells, int cap) {
+  static const int opts[] = {2, 4, 7, 8};
+  for (int c : opts) {
+    if (c > cap) break;
+    if (32 * c - 1 >= ly_cells) return c;
+  }
+  return cap;
+}
+
+int plan_fwd(bool pde, int nX, int LX, int nY, int LY, int d, int dtype, int n_levels,
+             int order_or_dyadic, int difference, int pairs_mode, int n_list,
+             FwdPlan& pl) {
+  if (dtype != KSIG_DTYPE_F32 && dtype != KSIG_DTYPE_F64)
+    return fail(KSIG_ERR_INVALID, "dtype must be KSIG_DTYPE_F32 or KSIG_DTYPE_F64");
+  if (nX <= 0 || LX <= 0 || d <= 0) return fail(KSIG_ERR_INVALID, "empty X (n=%d, L=%d, d=%d)", nX, LX, d);
+  if (pairs_mode == KSIG_PAIRS_UPPER || pairs_mode == KSIG_PAIRS_DIAG) { nY = nX; LY = LX; }
+  else if (nY <= 0 || LY <= 0) return fail(KSIG_ERR_INVALID, "empty Y (n=%d, L=%d)", nY, LY);
+  if (pairs_mode < 0 || pairs_mode > KSIG_PAIRS_LIST) return fail(KSIG_ERR_INVALID, "bad pairs_mode %d", pairs_mode);
+  const long long np = num_pairs(pairs_mode, nX, nY, n_list);
+  if (np < 0 || np > (long long)0x7fffffff) return fail(KSIG_ERR_INVALID, "pair count %lld out of range", np);
+  pl = FwdPlan{};
+  pl.f64 = dtype == KSIG_DTYPE_F64;
+  pl.diff = difference ? 1 : 0;
+  pl.ntasks = np;
+  int need_nl = 0, p = 0;
+  if (pde) {
+    if (order_or_dyadic < 0 || order_or_dyadic > 3)
+      return fail(KSIG_ERR_UNSUPPORTED, "dyadic_order %d not in [0, 3]", order_or_dyadic);
+    p = 1 << order_or_dyadic;
+    need_nl = 0;
+  } else {
+    if (n_levels <= 0) return fail(KSIG_ERR_INVALID, "n_levels must be positive");
+    int ord = order_or_dyadic;
+    ord = (ord <= 0 || ord >= n_levels) ? n_levels : ord;  // ksig/algorithms.py:37
+    p = ord;
+    need_nl = n_levels;
+  }
+  const int ly_cells = pl.diff ? LY - 1 : LY;
+  const int lx_cells = pl.diff ? LX - 1 : LX;
+  const int op = pde ? OP_PDE_FWD : OP_DP_FWD;
+  const int want = want_cols(ly_cells, 8);
+  const KernelEntry* k = find_kernel(op, pl.f64, d, want, need_nl, p, pl.diff);
+  if (!k)
+    return fail(KSIG_ERR_UNSUPPORTED,
+                "no compiled %s kernel for dtype=%s d=%d n_levels=%d order/F=%d difference=%d",
+                pde ? "PDE" : "DP", pl.f64 ? "f64" : "f32", d, n_levels, p, pl.diff);
+  pl.k = k;
+  pl.kd = k->kd;
+  pl.c = k->c;
+  pl.nl = k->nl;
+  pl.nl_out = need_nl;
+  pl.p = p;
+  pl.wpb = k->wpb;
+  const size_t es = pl.f64 ? 8 : 4;
+  pl.rs = round_up(pl.kd + 1, (int)(16 / es));
+  const int strip = pl.diff ? 32 * pl.c - 1 : 32 * pl.c;
+  pl.multi = ly_cells > strip ? 1 : 0;
+  if (pde) {
+    pl.nx_exchange = p;
+  } else {
+    int nh = 0;
+    for (int q = 2; q <= pl.nl; ++q) nh += q < p ? q : p;
+    pl.nx_exchange = nh > 0 ? nh : 1;
+  }
+  // Grid: one warp per SM slot, never more warps than pairs.
+  int occ = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k->func, k->wpb * 32, 0);
+  if (e != cudaSuccess || occ <= 0) occ = 1;
+  const int sms = sm_count() > 0 ? sm_count() : 148;
+  long long warps = (long long)sms * occ * k->wpb;
+  if (warps > np) warps = np > 0 ? np : 1;
+  pl.grid = (int)((warps + k->wpb - 1) / k->wpb);
+  const long long nwarps = (long long)pl.grid * k->wpb;
+  pl.rows_max = lx_cells > 32 ? lx_cells : 32;
+  pl.scratch_per_warp = pl.multi ? pl.rows_max * pl.nx_exchange : 0;
+  size_t off = 0;
+  pl.off_status = off; off = align_up(off + 16);
+  pl.off_xr = off; off = align_up(off + (size_t)nX * LX * pl.rs * es);
+  pl.off_yr = off; off = align_up(off + (size_t)nY * LY * pl.rs * es);
+  pl.off_xstart = off; off = align_up(off + (size_t)nX * 8);
+  pl.off_ystart = off; off = align_up(off + (size_t)nY * 8);
+  pl.off_xlen = off; off = align_up(off + (size_t)nX * 4);
+  pl.off_ylen = off; off = align_up(off + (size_t)nY * 4);
+  pl.off_scratch = off; off = align_up(off + (size_t)nwarps * pl.scratch_per_warp * es);
+  pl.total = off;
+  return KSIG_OK;
+}
+
+__global__ void starts_kernel(int64_t* start, int n, int L) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    start[i] = (int64_t)i * L;
+}
+
+template <typename T>
+int pack(const void* src, const int32_t* len, int n, int L, int d, int src_f64, int kind,
+         double param, int row_side, const FwdPlan& pl, T* dst, int64_t* start,
+         int32_t* len_out, int* status, cudaStream_t st) {
+  PackArgs a{src, len, n, L, d, src_f64, kind, param, row_side, pl.kd, pl.rs, len_out, status};
+  const long long total = (long long)n * L;
+  int blocks = (int)((total + 255) / 256);
+  if (blocks > 4096) blocks = 4096;
+  pack_rows_kernel<T><<<blocks, 256, 0, st>>>(a, dst);
+  KSIG_CUDA(cudaGetLastError());
+  starts_kernel<<<(n + 255) / 256 < 1024 ? (n + 255) / 256 : 1024, 256, 0, st>>>(start, n, L);
+  KSIG_CUDA(cudaGetLastError());
+  g_launches.fetch_add(2, std::memory_order_relaxed);
+  return KSIG_OK;
+}
+
+template <typename T>
+int run_fwd(const FwdPlan& pl, const void* X, const int32_t* lenX, int nX, int LX, const void* Y,
+            const int32_t* lenY, int nY, int LY, int d, int src_f64, int kind, double param,
+            int mode, const int32_t* list, double* out, char* ws, cudaStream_t st) {
+  int* status = reinterpret_cast<int*>(ws + pl.off_status);
+  T* xr = reinterpret_cast<T*>(ws + pl.off_xr);
+  T* yr = reinterpret_cast<T*>(ws + pl.off_yr);
+  int64_t* xs = reinterpret_cast<int64_t*>(ws + pl.off_xstart);
+  int64_t* ys = reinterpret_cast<int64_t*>(ws + pl.off_ystart);
+  int32_t* xl = reinterpret_cast<int32_t*>(ws + pl.off_xlen);
+  int32_t* yl = reinterpret_cast<int32_t*>(ws + pl.off_ylen);
+  const bool self = mode == KSIG_PAIRS_UPPER || mode == KSIG_PAIRS_DIAG;
+  int rc = pack<T>(X, lenX, nX, LX, d, src_f64, kind, param, 1, pl, xr, xs, xl, status, st);
+  if (rc) return rc;
+  if (self) rc = pack<T>(X, lenX, nX, LX, d, src_f64, kind, param, 0, pl, yr, ys, yl, status, st);
+  else rc = pack<T>(Y, lenY, nY, LY, d, src_f64, kind, param, 0, pl, yr, ys, yl, status, st);
+  if (rc) return rc;
+  SweepArgs<T> a{};
+  a.xr = xr; a.xstart = xs; a.xlen = xl;
+  a.yr = yr; a.ystart = ys; a.ylen = yl;
+  a.mode = mode;
+  a.nY = self ? nX : nY;
+  a.list = reinterpret_cast<const int2*>(list);
+  a.order = nullptr;
+  a.ntasks = (int)pl.ntasks;
+  a.kind = kind;
+  a.out = out;
+  a.scratch = pl.multi ? reinterpret_cast<T*>(ws + pl.off_scratch) : nullptr;
+  a.scratch_per_warp = pl.scratch_per_warp;
+  a.multi_strip = pl.multi;
+  a.nl_out = pl.nl_out;
+  a.nX = nX;
+  a.nYseq = self ? nX : nY;
+  a.status = status;
+  void* kargs[] = {&a};
+  KSIG_CUDA(launch_main(pl.k->func, dim3(pl.grid), dim3(pl.k->wpb * 32), kargs, st));
+  return KSIG_OK;
+}
+
+int check_common(const void* X, const void* Y, int pairs_mode, const int32_t* list, int n_list,
+                 int static_kind, double static_param) {
+  if (!X) return fail(KSIG_ERR_INVALID, "X is NULL");
+  if ((pairs_mode == KSIG_PAIRS_FULL || pairs_mode == KSIG_PAIRS_LIST) && !Y)
+    return fail(KSIG_ERR_INVALID, "Y is NULL");
+  if (pairs_mode == KSIG_PAIRS_LIST && (!list || n_list < 0))
+    return fail(KSIG_ERR_INVALID, "pair list missing");
+  if (static_kind != KSIG_STATIC_RBF && static_kind != KSIG_STATIC_LINEAR)
+    return fail(KSIG_ERR_INVALID, "unknown static kernel %d", static_kind);
+  if (!(static_param > 0))  // ksig/utils.py:33-34 (check_positive_value)
+    return fail(KSIG_ERR_INVALID, "The parameter '%s' should have a positive value.",
+                static_kind == KSIG_STATIC_RBF ? "bandwidth" : "scale");
+  return KSIG_OK;
+}
+
+int fwd_entry(bool pde, const void* X, const int32_t* lenX, int nX, int LX, const void* Y,
+              const int32_t* lenY, int nY, int LY, int d, int dtype, int static_kind,
+              double static_param, int n_levels, int order_or_dyadic, int difference,
+              int pairs_mode, const int32_t* list, int n_list, double* out, void* ws,
+              size_t ws_bytes, void* stream) {
+  int rc = check_common(X, Y, pairs_mode, list, n_list, static_kind, static_param);
+  if (rc) return rc;
+  if (!out) return fail(KSIG_ERR_INVALID, "output is NULL");
+  FwdPlan pl;
+  rc = plan_fwd(pde, nX, LX, nY, LY, d, dtype, n_levels, order_or_dyadic, difference, pairs_mode,
+                n_list, pl);
+  if (rc) return rc;
+  if (!ws || ws_bytes < pl.total)
+    return fail(KSIG_ERR_WORKSPACE, "workspace of %zu bytes is smaller than the %zu required",
+                ws_bytes, pl.total);
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  KSIG_CUDA(cudaMemsetAsync(ws, 0, 16, st));  // device status word
+  if (pl.ntasks == 0) return KSIG_OK;
+  if (pairs_mode == KSIG_PAIRS_UPPER || pairs_mode == KSIG_PAIRS_DIAG) { nY = nX; LY = LX; Y = X; lenY = lenX; }
+  const int f64 = dtype == KSIG_DTYPE_F64;
+  if (f64)
+    return run_fwd<double>(pl, X, lenX, nX, LX, Y, lenY, nY, LY, d, 1, static_kind, static_param,
+                           pairs_mode, list, out, static_cast<char*>(ws), st);
+  return run_fwd<float>(pl, X, lenX, nX, LX, Y, lenY, nY, LY, d, 0, static_kind, static_param,
+                        pairs_mode, list, out, static_cast<char*>(ws), st);
+}
+
+// FP32 FMA throughput probe: 8 independent FMA chains per thread.
+__global__ void fp32_probe_kernel(float* out, int iters, float a, float b) {
+  float v[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = threadIdx.x * 1e-3f + i;
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = fmaf(v[i], a, b);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) s += v[i];
+  if (s == 12345.678f) out[0] = s;  // keeps the chains live
+}
+
+}  // namespace
+}  // namespace ksig
+
+using namespace ksig;
+
+extern "C" {
+
+const char* ksig_version(void) { return "ksig_b200 0.1.0 (sm_100a)"; }
+
+size_t ksig_last_error(char* buf, size_t n) {
+  if (buf && n) {
+    size_t m = g_err.size() < n - 1 ? g_err.size() : n - 1;
+    memcpy(buf, g_err.data(), m);
+    buf[m] = 0;
+  }
+  return g_err.size();
+}
+
+long long ksig_num_pairs(int pairs_mode, int nX, int nY, int n_list) {
+  return num_pairs(pairs_mode, nX, nY, n_list);
+}
+
+size_t ksig_signature_kern_workspace(int nX, int LX, int nY, int LY, int d, int dtype,
+                                     int n_levels, int order, int difference, int pairs_mode,
+                                     int n_list) {
+  FwdPlan pl;
+  if (plan_fwd(false, nX, LX, nY, LY, d, dtype, n_levels, order, difference, pairs_mode, n_list,
+               pl))
+    return 0;
+  return pl.total;
+}
+
+int ksig_signature_kern(const void* X, const int32_t* lenX, int nX, int LX, const void* Y,
+                        const int32_t* lenY, int nY, int LY, int d, int dtype, int static_kind,
+                        double static_param, int n_levels, int order, int difference,
+                        int pairs_mode, const int32_t* pair_list, int n_list, double* out_levels,
+                        void* workspace, size_t workspace_bytes, void* stream) {
+  return fwd_entry(false, X, lenX, nX, LX, Y, lenY, nY, LY, d, dtype, static_kind, static_param,
+                   n_levels, order, difference, pairs_mode, pair_list, n_list, out_levels,
+                   workspace, workspace_bytes, stream);
+}
+
+size_t ksig_signature_kern_pde_workspace(int nX, int LX, int nY, int LY, int d, int dtype,
+                                         int dyadic_order, int difference, int pairs_mode,
+                                         int n_list) {
+  FwdPlan pl;
+  if (plan_fwd(true, nX, LX, nY, LY, d, dtype, 0, dyadic_order, difference, pairs_mode, n_list,
+               pl))
+    return 0;
+  return pl.total;
+}
+
+int ksig_signature_kern_pde(const void* X, const int32_t* lenX, int nX, int LX, const void* Y,
+                            const int32_t* lenY, int nY, int LY, int d, int dtype,
+                            int static_kind, double static_param, int dyadic_order,
+                            int difference, int pairs_mode, const int32_t* pair_list, int n_list,
+                            double* out, void* workspace, size_t workspace_bytes, void* stream) {
+  return fwd_entry(true, X, lenX, nX, LX, Y, lenY, nY, LY, d, dtype, static_kind, static_param,
+                   0, dyadic_order, difference, pairs_mode, pair_list, n_list, out, workspace,
+                   workspace_bytes, stream);
+}
+
+int ksig_normalize_levels(const double* levels, int n_lev, int pairs_mode, int nX, int nY,
+                          const double* diagX, const double* diagY, int normalize, void* out,
+                          int out_dtype, void* stream) {
+  if (!levels || !out) return fail(KSIG_ERR_INVALID, "NULL levels/out");
+  if (n_lev <= 0 || nX <= 0) return fail(KSIG_ERR_INVALID, "bad sizes");
+  if (pairs_mode != KSIG_PAIRS_FULL && pairs_mode != KSIG_PAIRS_UPPER)
+    return fail(KSIG_ERR_INVALID, "normalize needs FULL or UPPER pairs");
+  if (pairs_mode == KSIG_PAIRS_UPPER) nY = nX;
+  if (nY <= 0) return fail(KSIG_ERR_INVALID, "bad nY");
+  if (normalize && !diagX && pairs_mode == KSIG_PAIRS_FULL && nX != nY)
+    return fail(KSIG_ERR_INVALID, "diagX is required for a rectangular FULL Gram");
+  if (out_dtype != KSIG_DTYPE_F32 && out_dtype != KSIG_DTYPE_F64)
+    return fail(KSIG_ERR_INVALID, "bad out dtype");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  NormArgs a{levels, n_lev, pairs_mode, nX, nY, diagX, diagY ? diagY : diagX, normalize};
+  const long long total = (long long)nX * nY;
+  int blocks = (int)((total + 255) / 256);
+  if (blocks > 8192) blocks = 8192;
+  if (out_dtype == KSIG_DTYPE_F64) normalize_kernel<double><<<blocks, 256, 0, st>>>(a, (double*)out);
+  else normalize_kernel<float><<<blocks, 256, 0, st>>>(a, (float*)out);
+  KSIG_CUDA(cudaGetLastError());
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return KSIG_OK;
+}
+
+unsigned long long ksig_launch_count(void) { return g_launches.load(); }
+
+void ksig_profile_enable(int on) {
+  Profiler& P = prof();
+  std::lock_guard<std::mutex> lk(P.mu);
+  P.on = on != 0;
+}
+
+int ksig_profile_read(double* total_ms, long long* launches) {
+  Profiler& P = prof();
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+  {
+    std::lock_guard<std::mutex> lk(P.mu);
+    ev.swap(P.pending);
+  }
+  double tot = 0.0;
+  for (auto& e : ev) {
+    KSIG_CUDA(cudaEventSynchronize(e.second));
+    float ms = 0.f;
+    KSIG_CUDA(cudaEventElapsedTime(&ms, e.first, e.second));
+    tot += ms;
+  }
+  {
+    std::lock_guard<std::mutex> lk(P.mu);
+    for (auto& e : ev) P.pool.push_back(e);
+  }
+  if (total_ms) *total_ms = tot;
+  if (launches) *launches = (long long)ev.size();
+  return KSIG_OK;
+}
+
+int ksig_fp32_peak(double* tflops, void* stream) {
+  if (!tflops) return fail(KSIG_ERR_INVALID, "NULL output");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const int sms = sm_count() > 0 ? sm_count() : 148;
+  const int blocks = sms * 8, threads = 256, iters = 4096;
+  cudaEvent_t a, b;
+  KSIG_CUDA(cudaEventCreate(&a));
+  KSIG_CUDA(cudaEventCreate(&b));
+  float best = 1e30f;
+  for (int rep = 0; rep < 4; ++rep) {
+    KSIG_CUDA(cudaEventRecord(a, st));
+    fp32_probe_kernel<<<blocks, threads, 0, st>>>(nullptr, iters, 0.999f, 1e-3f);
+    KSIG_CUDA(cudaGetLastError());
+    KSIG_CUDA(cudaEventRecord(b, st));
+    KSIG_CUDA(cudaEventSynchronize(b));
+    float ms = 0.f;
+    KSIG_CUDA(cudaEventElapsedTime(&ms, a, b));
+    if (rep > 0 && ms < best) best = ms;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  const double flops = 2.0 * 8.0 * (double)iters * blocks * threads;
+  *tflops = flops / (best * 1e-3) / 1e12;
+  return KSIG_OK;
+}
+
+int ksig_workspace_status(void* workspace, void* stream) {
+  if (!workspace) return fail(KSIG_ERR_INVALID, "NULL workspace");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  int h = 0;
+  KSIG_CUDA(cudaMemcpyAsync(&h, workspace, sizeof(int), cudaMemcpyDeviceToHost, st));
+  KSIG_CUDA(cudaStreamSynchronize(st));
+  if (h != 0) {
+    int z = 0;
+    KSIG_CUDA(cudaMemcpyAsync(workspace, &z, sizeof(int), cudaMemcpyHostToDevice, st));
+    KSIG_CUDA(cudaStreamSynchronize(st));
+    return fail(h == KSIG_ERR_INVALID ? KSIG_ERR_INVALID : KSIG_ERR_DEVICE,
+                "device-side check failed (code %d)", h);
+  }
+  return KSIG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,64 @@
+// Packing of input sequences into the fused-Gram row format.
+//
+// A static-kernel value between point x (row side) and point y (column side)
+// is evaluated by the hot kernels as ONE dot product of packed rows:
+//     arg = xr[KD] + yr[KD] + sum_{k<KD} xr[k] * yr[k]
+//   RBF    (ksig/static/kernels.py:258-260, ksig/utils.py:149-156):
+//          xr = (2a x, -a|x|^2), yr = (y, -a|y|^2), a = log2(e)/max(2s^2,1e-12)
+//          so arg = -a |x-y|^2 and M = exp2(arg) = exp(-|x-y|^2 / max(2s^2,eps)).
+//   linear (ksig/static/kernels.py:155): xr = (s x, 0), yr = (y, 0), M = arg.
+// Rows are padded with zeros to KD coordinates and to a 16-byte stride so the
+// kernels read them with vector loads.  Norms are formed in FP64.
+#pragma once
+
+#include "common.cuh"
+
+namespace ksig {
+
+struct PackArgs {
+  const void* src;      // [n, L, d] dense, dtype src_f64 ? double : float
+  const int32_t* len;   // [n] or nullptr (= L)
+  int n, L, d;
+  int src_f64;
+  int kind;             // KIND_RBF / KIND_LINEAR
+  double param;         // bandwidth or scale
+  int row_side;         // 1: x-side scaling, 0: y-side
+  int kd;               // padded coordinate count (>= d)
+  int stride;           // packed row stride in elements
+  int32_t* len_out;     // [n] resolved lengths (clamped to [1, L])
+  int* status;
+};
+
+template <typename T>
+__global__ void pack_rows_kernel(PackArgs a, T* __restrict__ dst) {
+  const long long total = (long long)a.n * a.L;
+  const double alpha = 1.4426950408889634 / fmax(2.0 * a.param * a.param, 1e-12);
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < total;
+       r += (long long)gridDim.x * blockDim.x) {
+    const int seq = (int)(r / a.L);
+    const int t = (int)(r - (long long)seq * a.L);
+    if (t == 0 && a.len_out) {
+      int l = a.len ? a.len[seq] : a.L;
+      if (l < 1 || l > a.L) set_status(a.status, KSIG_ERR_INVALID);
+      a.len_out[seq] = l < 1 ? 1 : (l > a.L ? a.L : l);
+    }
+    T* out = dst + r * a.stride;
+    double nrm = 0.0;
+    for (int k = 0; k < a.kd; ++k) {
+      double v = 0.0;
+      if (k < a.d) {
+        v = a.src_f64 ? ((const double*)a.src)[r * a.d + k]
+                      : (double)((const float*)a.src)[r * a.d + k];
+      }
+      nrm += v * v;
+      double o;
+      if (a.kind == KIND_RBF) o = a.row_side ? 2.0 * alpha * v : v;
+      else o = a.row_side ? a.param * v : v;
+      out[k] = (T)o;
+    }
+    out[a.kd] = (T)(a.kind == KIND_RBF ? -alpha * nrm : 0.0);
+    for (int k = a.kd + 1; k < a.stride; ++k) out[k] = (T)0;
+  }
+}
+
+}  // namespace ksig

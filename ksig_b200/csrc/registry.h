@@ -1,0 +1,30 @@
+// Table of compiled kernel instantiations, filled by the generated
+// translation units under csrc/gen/ (see build.py for the instance list).
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace ksig {
+
+enum KernelOp : int {
+  OP_DP_FWD = 0,   // SweepArgs<T>          dp_fwd_kernel
+  OP_PDE_FWD = 1,  // SweepArgs<T>          pde_fwd_kernel   (p = refinement F)
+  OP_DP_BWD = 2,   // DpBwdArgs<T>          dp_bwd_kernel
+  OP_PDE_BWD = 3,  // PdeBwdArgs<T>         pde_bwd_kernel
+};
+
+struct KernelEntry {
+  int op, f64, kd, c, nl, p, diff, wpb;
+  const void* func;
+};
+
+struct KernelTable {
+  const KernelEntry* entries;
+  int n;
+};
+
+// All tables (defined in the generated registry translation unit).
+extern const KernelTable kAllTables[];
+extern const int kNumTables;
+
+}  // namespace ksig

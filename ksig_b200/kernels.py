@@ -1,0 +1,214 @@
+"""Signature kernels with KSig's callable API, computed by sm_100a kernels.
+
+``SignatureKernel`` and ``SignaturePDEKernel`` keep the constructor and call
+semantics of ``ksig.kernels`` (ksig/kernels.py:25-256)::
+
+    K = SignatureKernel(n_levels=5, order=1, difference=True, normalize=True,
+                        n_features=None, static_kernel=RBFKernel(1.0))
+    K(X)                 # [nX, nX]
+    K(X, Y)              # [nX, nY]
+    K(X, diag=True)      # [nX]
+    K(X, Y, return_on_gpu=True)   # torch CUDA tensor instead of NumPy
+
+``X`` / ``Y`` may be NumPy arrays, PyTorch tensors (CPU or CUDA) of shape
+``[n, L, d]`` (or ``[n, L*d]`` with ``n_features``), or a list of ``[L_i, d]``
+arrays of different lengths (ragged; no reference counterpart — the result
+equals the reference on the edge-padded dense array).  The arithmetic runs
+in the input dtype (float32 -> FP32 kernels with FP64 reductions, float64 ->
+FP64).  Torch inputs that require grad (and an RBF ``bandwidth`` given as a
+tensor that requires grad) are differentiated through a hand-written
+adjoint.
+"""
+
+import warnings
+from typing import Optional
+
+import numpy as np
+import torch
+
+from . import _engine as E
+from . import _lib as L
+from . import static as static_mod
+from . import utils
+from .static.kernels import StaticKernel
+
+
+def _is_ragged(X):
+  return isinstance(X, (list, tuple))
+
+
+def _to_seqs(X, n_features, reset_obj=None):
+  """Validates and moves a batch of sequences to the device.
+
+  Mirrors ``SignatureBase._validate_data`` (ksig/kernels.py:56-90) for dense
+  inputs; ragged inputs (lists) are padded and carry their lengths.
+  Returns (Seqs, was_torch, requires_grad_tensor_or_None).
+  """
+  if _is_ragged(X):
+    seqs = [s if isinstance(s, torch.Tensor) else torch.as_tensor(np.asarray(s))
+            for s in X]
+    if not seqs:
+      raise ValueError('empty sequence list')
+    seqs = [s.reshape(s.shape[0], -1) if s.ndim != 2 else s for s in seqs]
+    d = seqs[0].shape[-1]
+    if any(s.shape[-1] != d for s in seqs):
+      raise ValueError('all sequences must have the same number of features')
+    if n_features is not None and d != n_features:
+      raise ValueError(
+          'Number of features in `X` does not match saved `n_features` param.')
+    dtype = seqs[0].dtype if seqs[0].dtype in (torch.float32, torch.float64) \
+        else torch.float64
+    lens = [max(int(s.shape[0]), 1) for s in seqs]
+    Lmax = max(lens)
+    data = torch.zeros((len(seqs), Lmax, d), dtype=dtype, device='cuda')
+    for i, s in enumerate(seqs):
+      if s.shape[0] > 0:
+        data[i, :s.shape[0]] = s.to(device='cuda', dtype=dtype)
+    lengths = torch.tensor(lens, dtype=torch.int32, device='cuda')
+    return E.Seqs(data, lengths), False, None
+  was_torch = isinstance(X, torch.Tensor)
+  if not was_torch:
+    X = torch.as_tensor(np.asarray(X))
+  if X.ndim == 2:
+    if n_features is None:
+      warnings.warn('`X` has ndim==2. Assuming inputs are univariate time '
+                    'series. Recommend passing an `n_features` parameter '
+                    'during init when using flattened arrays of ndim==2.')
+      n_features = 1
+  elif X.ndim == 3:
+    if n_features is None:
+      n_features = X.shape[-1]
+    elif X.shape[-1] != n_features:
+      raise ValueError(
+          'Number of features in `X` does not match saved `n_features` param.')
+  else:
+    raise ValueError(
+        'Only input sequence arrays with ndim==2 or ndim==3 are supported.')
+  X = X.reshape([X.shape[0], -1, n_features])
+  if X.dtype not in (torch.float32, torch.float64):
+    X = X.to(torch.float64)
+  grad_src = X if (was_torch and X.requires_grad) else None
+  Xd = X.detach().to('cuda').contiguous()
+  return E.Seqs(Xd), was_torch, grad_src
+
+
+class SignatureBase:
+  """Shared parameters and validation (ksig/kernels.py:25-90)."""
+
+  def __init__(self, n_levels: int = 5, order: int = 1,
+               difference: bool = True, normalize: bool = True,
+               n_features: Optional[int] = None):
+    self.n_levels = utils.check_positive_value(n_levels, 'n_levels')
+    self.order = (self.n_levels if order <= 0 or order >= self.n_levels
+                  else order)
+    self.normalize = normalize
+    self.difference = difference
+    self.n_features = (utils.check_positive_value(n_features, 'n_features')
+                       if n_features is not None else None)
+
+  def fit(self, X, y=None):
+    return self
+
+  def _static(self):
+    sk = self.static_kernel
+    if not isinstance(sk, StaticKernel) or sk.kind is None:
+      raise ValueError('static_kernel must be RBFKernel or LinearKernel')
+    return sk.kind, sk.param
+
+  def __call__(self, X, Y=None, diag: bool = False,
+               return_on_gpu: bool = False):
+    """Kernel matrix ``K(X, Y)``, ``K(X, X)`` or its diagonal
+    (``Kernel.__call__``, ksig/static/kernels.py:71-97)."""
+    if not torch.cuda.is_available():
+      raise RuntimeError('ksig_b200 needs a CUDA device (no CPU fallback)')
+    Xs, _, gx = _to_seqs(X, self.n_features)
+    Ys, gy = None, None
+    if not diag and Y is not None:
+      Ys, _, gy = _to_seqs(Y, self.n_features)
+    if diag:
+      K = self._Kdiag(Xs)
+    elif gx is not None or gy is not None or self._param_requires_grad():
+      K = self._K_autograd(X if gx is not None else None, Xs, gx,
+                           Ys, gy, Y is None)
+    else:
+      K = self._K(Xs, Ys)
+    if return_on_gpu:
+      return K
+    if K.requires_grad:
+      return K
+    return K.detach().cpu().numpy()
+
+  def _param_requires_grad(self):
+    p = getattr(self.static_kernel, 'bandwidth', None)
+    return isinstance(p, torch.Tensor) and p.requires_grad
+
+  def _K_autograd(self, *args):
+    raise NotImplementedError('gradients are not available for this kernel')
+
+
+class SignatureKernel(SignatureBase):
+  """Full-rank truncated signature kernel (ksig/kernels.py:97-214)."""
+
+  def __init__(self, n_levels: int = 5, order: int = 1,
+               difference: bool = True, normalize: bool = True,
+               n_features: Optional[int] = None,
+               static_kernel: Optional[StaticKernel] = None):
+    super().__init__(n_levels=n_levels, order=order, difference=difference,
+                     normalize=normalize, n_features=n_features)
+    self.static_kernel = static_kernel or static_mod.kernels.RBFKernel()
+
+  # -- level kernels ------------------------------------------------------
+  def _levels(self, Xs, Ys, mode):
+    kind, param = self._static()
+    return E.sig_levels(Xs, Ys, mode, self.n_levels, self.order,
+                        self.difference, kind, param)
+
+  def _Kdiag(self, Xs):
+    """ksig/kernels.py:166-178: ones when normalising."""
+    if self.normalize:
+      return torch.full((Xs.n,), 1., dtype=torch.float64,
+                        device=Xs.data.device)
+    lev = self._levels(Xs, None, L.PAIRS_DIAG)
+    return lev.sum(dim=0).to(Xs.data.dtype)
+
+  def _K(self, Xs, Ys=None):
+    """ksig/kernels.py:180-214 (levels -> per-level normalisation -> mean)."""
+    out_dtype = Xs.data.dtype
+    if Ys is None:
+      lev = self._levels(Xs, None, L.PAIRS_UPPER)
+      return E.normalize_levels(lev, L.PAIRS_UPPER, Xs.n, Xs.n, None, None,
+                                self.normalize, out_dtype)
+    lev = self._levels(Xs, Ys, L.PAIRS_FULL)
+    dx = dy = None
+    if self.normalize:
+      dx = self._levels(Xs, None, L.PAIRS_DIAG)
+      dy = self._levels(Ys, None, L.PAIRS_DIAG)
+    return E.normalize_levels(lev, L.PAIRS_FULL, Xs.n, Ys.n, dx, dy,
+                              self.normalize, out_dtype)
+
+
+class SignaturePDEKernel(SignatureKernel):
+  """Signature-PDE kernel (ksig/kernels.py:218-256).
+
+  ``dyadic_order`` (no reference counterpart; default 0 = the reference
+  scheme) refines every cell of the Goursat grid into 2^k x 2^k cells.
+  """
+
+  def __init__(self, difference: bool = True, normalize: bool = True,
+               n_features: Optional[int] = None,
+               static_kernel: Optional[StaticKernel] = None,
+               dyadic_order: int = 0):
+    self.difference = difference
+    self.normalize = normalize
+    self.n_features = (utils.check_positive_value(n_features, 'n_features')
+                       if n_features is not None else None)
+    self.static_kernel = static_kernel or static_mod.kernels.RBFKernel()
+    if int(dyadic_order) < 0:
+      raise ValueError('dyadic_order must be non-negative')
+    self.dyadic_order = int(dyadic_order)
+
+  def _levels(self, Xs, Ys, mode):
+    kind, param = self._static()
+    v = E.pde_values(Xs, Ys, mode, self.dyadic_order, self.difference, kind,
+                     param)
+    return v[None, :]
