@@ -36,7 +36,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
   sys.path.insert(0, ROOT)
 
-N_SEQ = 512
+N_SEQ = 512       # sequences per side (--n-seq shrinks it for profiling only)
 SEQ_LEN = 200
 D_WALK = 8
 N_LEVELS = 5
@@ -339,7 +339,11 @@ def main():
   ap.add_argument('--cpu-pairs', type=int, default=40)
   ap.add_argument('--ref-pairs', type=int, default=32)
   ap.add_argument('--no-cpu', action='store_true')
+  ap.add_argument('--n-seq', type=int, default=N_SEQ,
+                  help='sequences per side; smaller values are for profiling '
+                       'captures only, not bench lines')
   args = ap.parse_args()
+  globals()['N_SEQ'] = args.n_seq
   args.warmup = max(args.warmup, 3)
   world = int(os.environ.get('WORLD_SIZE', '1'))
   rank = int(os.environ.get('RANK', '0'))

@@ -208,7 +208,7 @@ int plan_fwd(bool pde, int nX, int LX, int nY, int LY, int d, int dtype, int n_l
   const int strip = pl.diff ? 32 * pl.c - 1 : 32 * pl.c;
   pl.multi = ly_cells > strip ? 1 : 0;
   if (pde) {
-    pl.nx_exchange = p;
+    pl.nx_exchange = 2 * p;
   } else {
     int nh = 0;
     for (int q = 2; q <= pl.nl; ++q) nh += q < p ? q : p;
