@@ -129,6 +129,34 @@ int ksig_signature_kern_pde(const void* X, const int32_t* lenX, int nX,
                             double* out, void* workspace,
                             size_t workspace_bytes, void* stream);
 
+/* Workspace (bytes) required by ksig_signature_kern_bwd. */
+size_t ksig_signature_kern_bwd_workspace(int nX, int LX, int nY, int LY,
+                                         int d, int dtype, int n_levels,
+                                         int order, int difference,
+                                         int pairs_mode, int n_list);
+
+/*
+ * Adjoint of ksig_signature_kern (no reference counterpart: the reference
+ * has no gradients).  For every pair p = (a, b) of the enumeration and
+ * grad_levels[k, p] = dL/dlevel_k(p) (float64 [n_levels + 1, P], row 0
+ * ignored) it accumulates
+ *   dX[a]   += sum_k grad_levels[k, p] * d level_k(x_a, y_b) / d x_a
+ *   *dparam += sum_k grad_levels[k, p] * d level_k(x_a, y_b) / d param
+ * dX has X's dtype and shape [nX, LX, d] and is NOT cleared; only the ROW
+ * sequence of each pair is differentiated (call again with the roles
+ * swapped for the column side).  dparam (float64 scalar, may be NULL) is the
+ * RBF bandwidth or the linear scale.  difference must be 1.
+ */
+int ksig_signature_kern_bwd(const void* X, const int32_t* lenX, int nX,
+                            int LX, const void* Y, const int32_t* lenY,
+                            int nY, int LY, int d, int dtype,
+                            int static_kind, double static_param,
+                            int n_levels, int order, int difference,
+                            int pairs_mode, const int32_t* pair_list,
+                            int n_list, const double* grad_levels, void* dX,
+                            double* dparam, void* workspace,
+                            size_t workspace_bytes, void* stream);
+
 /*
  * Normalisation and level mean (replaces ksig/kernels.py:190-214).
  *   levels   float64 [n_lev, P] from one of the calls above with pairs_mode

@@ -81,6 +81,38 @@ def sig_levels(X, Y, mode, n_levels, order, difference, kind, param,
   return out
 
 
+def sig_levels_bwd(X, Y, mode, n_levels, order, kind, param, grad_levels,
+                   dX=None, want_dparam=True, pair_list=None):
+  """Row-side adjoint of :func:`sig_levels`.
+
+  Accumulates into ``dX`` (``[nX, LX, d]``, X's dtype; allocated as zeros
+  when None) and returns ``(dX, dparam)`` where dparam is a float64 device
+  scalar (or None).
+  """
+  lib = L.lib()
+  Yv = X if Y is None else Y
+  dt = _dtype_code(X.data)
+  n_list = 0 if pair_list is None else pair_list.shape[0]
+  if dX is None:
+    dX = torch.zeros_like(X.data)
+  dpar = torch.zeros((1,), dtype=torch.float64, device=X.data.device) \
+      if want_dparam else None
+  gl = grad_levels.to(torch.float64).contiguous()
+  ws_bytes = lib.ksig_signature_kern_bwd_workspace(
+      X.n, X.L, Yv.n, Yv.L, X.d, dt, n_levels, order, 1, mode, n_list)
+  if ws_bytes == 0:
+    L.check(L.ERR_UNSUPPORTED if 'no compiled' in L.last_error()
+            else L.ERR_INVALID)
+  ws = _workspace(ws_bytes, X.data.device)
+  rc = lib.ksig_signature_kern_bwd(
+      _ptr(X.data), _ptr(X.lengths), X.n, X.L, _ptr(Yv.data),
+      _ptr(Yv.lengths), Yv.n, Yv.L, X.d, dt, kind, float(param), n_levels,
+      order, 1, mode, _ptr(pair_list), n_list, _ptr(gl), _ptr(dX),
+      _ptr(dpar), _ptr(ws), ws_bytes, _stream())
+  L.check(rc)
+  return dX, dpar
+
+
 def pde_values(X, Y, mode, dyadic_order, difference, kind, param,
                pair_list=None):
   """Signature-PDE kernel per pair ``[P]`` (float64)."""
@@ -129,3 +161,9 @@ def to_numpy(t):
 
 def np_dtype(t):
   return np.float64 if t.dtype == torch.float64 else np.float32
+
+
+def pde_values_bwd(X, Y, mode, dyadic_order, kind, param, grad, dX=None,
+                   want_dparam=True, pair_list=None):
+  """Row-side adjoint of :func:`pde_values` (see ksig_signature_kern_pde_bwd)."""
+  raise NotImplementedError('the PDE adjoint is not built into this library')

@@ -32,7 +32,7 @@ NVCC_FLAGS = ['-O3', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC',
               '-Xcompiler', '-O2', '--expt-relaxed-constexpr', '-ftz=true']
 WPB = 4  # warps per block of the sweep kernels
 
-KD_ALL = [2, 4, 6, 8, 10, 12, 16, 24, 32]
+KD_ALL = [2, 4, 6, 8, 9, 10, 12, 16, 24, 32]
 KD_FEW = [4, 8, 16, 32]
 NL_ALL = [1, 2, 3, 4, 5, 6, 8]
 
@@ -68,12 +68,22 @@ def instances():
   for dt in ('f32', 'f64'):
     for f, kd in itertools.product([1, 2, 4], KD_FEW):
       add(('pde', dt, kd, 2, 0, f, 0))
+  # DP backward (row-side gradients).
+  for dt, cs in (('f32', [2, 4]), ('f64', [2])):
+    for nl, kd, c in itertools.product(NL_ALL, KD_ALL, cs):
+      add(('dpb', dt, kd, c, nl, 1, 1))
+    for nl, kd in itertools.product([2, 3, 4, 5, 6, 8], KD_ALL):
+      add(('dpb', dt, kd, 2, nl, 2, 1))
+    for p, nls in ((3, [3, 4, 5, 6, 8]), (4, [4, 5, 6, 8])):
+      for nl, kd in itertools.product(nls, KD_FEW):
+        add(('dpb', dt, kd, 2, nl, p, 1))
   return out
 
 
 OPS = {
     'dp': ('OP_DP_FWD', 'dp_fwd_kernel<{T}, {kd}, {c}, {nl}, {p}, {diff}, {wpb}>'),
     'pde': ('OP_PDE_FWD', 'pde_fwd_kernel<{T}, {kd}, {c}, {p}, {diff}, {wpb}>'),
+    'dpb': ('OP_DP_BWD', 'dp_bwd_kernel<{T}, {kd}, {c}, {nl}, {p}, {wpb}>'),
 }
 
 
@@ -92,7 +102,8 @@ def generate():
   tables = []
   for key, insts in sorted(groups.items()):
     lines = ['// Generated by ksig_b200/build.py; do not edit.',
-             '#include "../sweep.cuh"', '#include "../registry.h"',
+             '#include "../sweep.cuh"', '#include "../dp_bwd.cuh"',
+             '#include "../registry.h"',
              'namespace ksig {']
     ents = []
     for op, dt, kd, c, nl, p, diff in insts:

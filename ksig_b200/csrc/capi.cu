@@ -3,6 +3,7 @@
 // include/ksig_b200.h.
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <atomic>
 #include <mutex>
@@ -14,6 +15,7 @@
 #include "pack.cuh"
 #include "registry.h"
 #include "sweep.cuh"
+#include "dp_bwd.cuh"
 
 namespace ksig {
 namespace {
@@ -54,9 +56,30 @@ Profiler& prof() {
   return p;
 }
 
+// Dynamic shared memory of a sweep kernel: one staging slot of C packed rows
+// per lane (SweepSmem in sweep.cuh).
+size_t sweep_dyn_smem_bytes(int wpb, int c, int rs, size_t es) {
+  return (size_t)wpb * 32 * c * rs * es;
+}
+
+// Raises the kernel's dynamic shared-memory limit once per (device, kernel).
+cudaError_t ensure_smem_attr(const void* func, size_t bytes) {
+  static std::mutex mu;
+  static std::vector<std::pair<std::pair<int, const void*>, size_t>> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  for (auto& d : done)
+    if (d.first.first == dev && d.first.second == func && d.second >= bytes) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) done.push_back({{dev, func}, bytes});
+  return e;
+}
+
 // Launches `func` and, when profiling is on, brackets it with CUDA events on
 // the same stream.
-cudaError_t launch_main(const void* func, dim3 grid, dim3 block, void** args, cudaStream_t st) {
+cudaError_t launch_main(const void* func, dim3 grid, dim3 block, void** args, size_t smem,
+                        cudaStream_t st) {
   Profiler& P = prof();
   std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
   bool timed = false;
@@ -74,7 +97,7 @@ cudaError_t launch_main(const void* func, dim3 grid, dim3 block, void** args, cu
     }
   }
   if (timed) cudaEventRecord(ev.first, st);
-  cudaError_t e = cudaLaunchKernel(func, grid, block, args, 0, st);
+  cudaError_t e = cudaLaunchKernel(func, grid, block, args, smem, st);
   g_launches.fetch_add(1, std::memory_order_relaxed);
   if (timed) {
     cudaEventRecord(ev.second, st);
@@ -132,6 +155,7 @@ struct FwdPlan {
   int f64, kd, rs, c, nl, nl_out, p, diff, nx_exchange;
   long long ntasks;
   int multi, grid, wpb;
+  size_t dyn_smem;
   long long rows_max, scratch_per_warp;
   size_t off_status, off_xr, off_yr, off_xstart, off_ystart, off_xlen, off_ylen,
       off_scratch, total;
@@ -148,9 +172,19 @@ long long num_pairs(int mode, int nX, int nY, int n_list) {
   return -1;
 }
 
+// Integer tuning override from the environment (unset -> def).
+int env_int(const char* name, int def) {
+  const char* v = getenv(name);
+  if (!v || !*v) return def;
+  return atoi(v);
+}
+
 // Column count per lane: smallest c whose strip covers the longest column
 // sequence in one strip, capped by what the register budget allows.
+// KSIG_FWD_COLS overrides the choice (tuning).
 int want_cols(int ly_cells, int cap) {
+  const int forced = env_int("KSIG_FWD_COLS", 0);
+  if (forced > 0) return forced;
   static const int opts[] = {2, 4, 7, 8};
   for (int c : opts) {
     if (c > cap) break;
@@ -215,8 +249,11 @@ int plan_fwd(bool pde, int nX, int LX, int nY, int LY, int d, int dtype, int n_l
     pl.nx_exchange = nh > 0 ? nh : 1;
   }
   // Grid: one warp per SM slot, never more warps than pairs.
+  pl.dyn_smem = sweep_dyn_smem_bytes(k->wpb, pl.c, pl.rs, es);
+  cudaError_t e = ensure_smem_attr(k->func, pl.dyn_smem);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(MaxDynamicSharedMemorySize)");
   int occ = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k->func, k->wpb * 32, 0);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k->func, k->wpb * 32, pl.dyn_smem);
   if (e != cudaSuccess || occ <= 0) occ = 1;
   const int sms = sm_count() > 0 ? sm_count() : 148;
   long long warps = (long long)sms * occ * k->wpb;
@@ -294,7 +331,104 @@ int run_fwd(const FwdPlan& pl, const void* X, const int32_t* lenX, int nX, int L
   a.nYseq = self ? nX : nY;
   a.status = status;
   void* kargs[] = {&a};
-  KSIG_CUDA(launch_main(pl.k->func, dim3(pl.grid), dim3(pl.k->wpb * 32), kargs, st));
+  KSIG_CUDA(launch_main(pl.k->func, dim3(pl.grid), dim3(pl.k->wpb * 32), kargs, pl.dyn_smem, st));
+  return KSIG_OK;
+}
+
+// Backward: the forward's packing layout plus per-warp scratch for strip
+// carries and per-strip column sums (dp_bwd.cuh).
+struct BwdPlan {
+  FwdPlan f;
+  const KernelEntry* k;
+  int c, nx, ns_max, rows_max, grid;
+  long long scratch_per_warp;
+  size_t off_scratch, total;
+};
+
+int plan_bwd(int nX, int LX, int nY, int LY, int d, int dtype, int n_levels, int order,
+             int difference, int pairs_mode, int n_list, BwdPlan& bp) {
+  int rc = plan_fwd(false, nX, LX, nY, LY, d, dtype, n_levels, order, difference, pairs_mode,
+                    n_list, bp.f);
+  if (rc) return rc;
+  if (!difference)
+    return fail(KSIG_ERR_UNSUPPORTED, "gradients need difference=True");
+  if (pairs_mode == KSIG_PAIRS_UPPER || pairs_mode == KSIG_PAIRS_DIAG) { nY = nX; LY = LX; }
+  const int ly = LY - 1, lx = LX - 1;
+  const int forced = env_int("KSIG_BWD_COLS", 0);
+  int want = forced > 0 ? forced : (ly <= 63 ? 2 : 4);
+  const KernelEntry* k = find_kernel(OP_DP_BWD, bp.f.f64, d, want, n_levels, bp.f.p, 1);
+  if (!k)
+    return fail(KSIG_ERR_UNSUPPORTED, "no compiled DP backward kernel for dtype=%s d=%d "
+                "n_levels=%d order=%d", bp.f.f64 ? "f64" : "f32", d, n_levels, bp.f.p);
+  bp.k = k;
+  bp.c = k->c;
+  int nh = 0;
+  for (int q = 2; q <= k->nl; ++q) nh += q < bp.f.p ? q : bp.f.p;
+  bp.nx = nh > 0 ? nh : 1;
+  const int strip = 32 * bp.c - 1;
+  bp.ns_max = ly <= strip ? 1 : (ly + strip - 1) / strip;
+  bp.rows_max = lx > 1 ? lx : 1;
+  int occ = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k->func, k->wpb * 32, 0);
+  if (e != cudaSuccess || occ <= 0) occ = 1;
+  const int sms = sm_count() > 0 ? sm_count() : 148;
+  long long warps = (long long)sms * occ * k->wpb;
+  if (warps > bp.f.ntasks) warps = bp.f.ntasks > 0 ? bp.f.ntasks : 1;
+  bp.grid = (int)((warps + k->wpb - 1) / k->wpb);
+  const size_t es = bp.f.f64 ? 8 : 4;
+  bp.scratch_per_warp = bp.ns_max > 1
+      ? ((long long)bp.ns_max * bp.rows_max + bp.rows_max) * bp.nx +
+            (long long)bp.ns_max * 32 * bp.nx * bp.c
+      : 0;
+  bp.off_scratch = bp.f.off_scratch;  // the forward scratch region is unused here
+  bp.total = align_up(bp.off_scratch + (size_t)bp.grid * k->wpb * bp.scratch_per_warp * es);
+  if (bp.total < bp.f.total) bp.total = bp.f.total;
+  return KSIG_OK;
+}
+
+template <typename T>
+int run_bwd(const BwdPlan& bp, const void* X, const int32_t* lenX, int nX, int LX,
+            const void* Y, const int32_t* lenY, int nY, int LY, int d, int src_f64, int kind,
+            double param, int mode, const int32_t* list, const double* glev, int nl_out,
+            void* dX, double* dparam, char* ws, cudaStream_t st) {
+  const FwdPlan& pl = bp.f;
+  int* status = reinterpret_cast<int*>(ws + pl.off_status);
+  T* xr = reinterpret_cast<T*>(ws + pl.off_xr);
+  T* yr = reinterpret_cast<T*>(ws + pl.off_yr);
+  int64_t* xs = reinterpret_cast<int64_t*>(ws + pl.off_xstart);
+  int64_t* ys = reinterpret_cast<int64_t*>(ws + pl.off_ystart);
+  int32_t* xl = reinterpret_cast<int32_t*>(ws + pl.off_xlen);
+  int32_t* yl = reinterpret_cast<int32_t*>(ws + pl.off_ylen);
+  const bool self = mode == KSIG_PAIRS_UPPER || mode == KSIG_PAIRS_DIAG;
+  int rc = pack<T>(X, lenX, nX, LX, d, src_f64, kind, param, 1, pl, xr, xs, xl, status, st);
+  if (rc) return rc;
+  if (self) rc = pack<T>(X, lenX, nX, LX, d, src_f64, kind, param, 0, pl, yr, ys, yl, status, st);
+  else rc = pack<T>(Y, lenY, nY, LY, d, src_f64, kind, param, 0, pl, yr, ys, yl, status, st);
+  if (rc) return rc;
+  DpBwdArgs<T> a{};
+  a.xr = xr; a.xstart = xs; a.xlen = xl;
+  a.yr = yr; a.ystart = ys; a.ylen = yl;
+  a.mode = mode;
+  a.nY = self ? nX : nY;
+  a.list = reinterpret_cast<const int2*>(list);
+  a.ntasks = (int)pl.ntasks;
+  a.nX = nX;
+  a.nYseq = self ? nX : nY;
+  a.kind = kind;
+  a.param = param;
+  a.glev = glev;
+  a.nl_out = nl_out;
+  a.dX = reinterpret_cast<T*>(dX);
+  a.LX = LX;
+  a.d = d;
+  a.dparam = dparam;
+  a.scratch = bp.scratch_per_warp ? reinterpret_cast<T*>(ws + bp.off_scratch) : nullptr;
+  a.scratch_per_warp = bp.scratch_per_warp;
+  a.ns_max = bp.ns_max;
+  a.rows_max = bp.rows_max;
+  a.status = status;
+  void* kargs[] = {&a};
+  KSIG_CUDA(launch_main(bp.k->func, dim3(bp.grid), dim3(bp.k->wpb * 32), kargs, 0, st));
   return KSIG_OK;
 }
 
@@ -415,6 +549,43 @@ int ksig_signature_kern_pde(const void* X, const int32_t* lenX, int nX, int LX, 
   return fwd_entry(true, X, lenX, nX, LX, Y, lenY, nY, LY, d, dtype, static_kind, static_param,
                    0, dyadic_order, difference, pairs_mode, pair_list, n_list, out, workspace,
                    workspace_bytes, stream);
+}
+
+size_t ksig_signature_kern_bwd_workspace(int nX, int LX, int nY, int LY, int d, int dtype,
+                                         int n_levels, int order, int difference,
+                                         int pairs_mode, int n_list) {
+  BwdPlan bp;
+  if (plan_bwd(nX, LX, nY, LY, d, dtype, n_levels, order, difference, pairs_mode, n_list, bp))
+    return 0;
+  return bp.total;
+}
+
+int ksig_signature_kern_bwd(const void* X, const int32_t* lenX, int nX, int LX, const void* Y,
+                            const int32_t* lenY, int nY, int LY, int d, int dtype,
+                            int static_kind, double static_param, int n_levels, int order,
+                            int difference, int pairs_mode, const int32_t* pair_list, int n_list,
+                            const double* grad_levels, void* dX, double* dparam,
+                            void* workspace, size_t workspace_bytes, void* stream) {
+  int rc = check_common(X, Y, pairs_mode, pair_list, n_list, static_kind, static_param);
+  if (rc) return rc;
+  if (!grad_levels || !dX) return fail(KSIG_ERR_INVALID, "grad_levels / dX is NULL");
+  BwdPlan bp;
+  rc = plan_bwd(nX, LX, nY, LY, d, dtype, n_levels, order, difference, pairs_mode, n_list, bp);
+  if (rc) return rc;
+  if (!workspace || workspace_bytes < bp.total)
+    return fail(KSIG_ERR_WORKSPACE, "workspace of %zu bytes is smaller than the %zu required",
+                workspace_bytes, bp.total);
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  KSIG_CUDA(cudaMemsetAsync(workspace, 0, 16, st));
+  if (bp.f.ntasks == 0) return KSIG_OK;
+  if (pairs_mode == KSIG_PAIRS_UPPER || pairs_mode == KSIG_PAIRS_DIAG) { nY = nX; LY = LX; Y = X; lenY = lenX; }
+  if (dtype == KSIG_DTYPE_F64)
+    return run_bwd<double>(bp, X, lenX, nX, LX, Y, lenY, nY, LY, d, 1, static_kind, static_param,
+                           pairs_mode, pair_list, grad_levels, n_levels, dX, dparam,
+                           static_cast<char*>(workspace), st);
+  return run_bwd<float>(bp, X, lenX, nX, LX, Y, lenY, nY, LY, d, 0, static_kind, static_param,
+                        pairs_mode, pair_list, grad_levels, n_levels, dX, dparam,
+                        static_cast<char*>(workspace), st);
 }
 
 int ksig_normalize_levels(const double* levels, int n_lev, int pairs_mode, int nX, int nY,

@@ -26,6 +26,8 @@
 // which makes their increments exactly zero (edge-padding invariance).
 #pragma once
 
+#include <cuda_pipeline.h>
+
 #include "common.cuh"
 
 namespace ksig {
@@ -58,8 +60,18 @@ struct ItemInfo {
   int task, Lx, Ly, s, ns;
 };
 
+// Smem slot per lane for the next item's column points (cp.async staging);
+// the kernels take WPB of these as dynamic shared memory
+// (sweep_dyn_smem_bytes on the host).
+template <typename T, int KD, int C>
+struct SweepSmem {
+  static constexpr int RS = packed_stride<T>(KD);
+  T ynext[32][C * RS];
+};
+
 template <typename T, int KD, int C, bool DIFF, int WPB, class Policy>
-__device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol) {
+__device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
+                                      SweepSmem<T, KD, C>& sm) {
   constexpr int NX = Policy::NX;
   constexpr int RS = packed_stride<T>(KD);
   constexpr int VN = Vec<T>::N;
@@ -70,59 +82,85 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol) {
   const long long wg = (long long)blockIdx.x * WPB + (threadIdx.x >> 5);
   const long long nw = (long long)gridDim.x * WPB;
   T* bbuf = args.scratch ? args.scratch + wg * args.scratch_per_warp : nullptr;
+  T* yslot = sm.ynext[lane];
 
-  long long seq = 0;
-  int task = -1, a = 0, b = 0, Lx = 1, Ly = 1, rows = 16, ns = 1, s = 0, u = 0;
-
-  auto load_task = [&](long long q, int& t_, int& a_, int& b_, int& Lx_,
-                       int& Ly_, int& rows_, int& ns_) {
+  // One item = one strip of one pair.
+  struct Item {
+    const T* xb;  // first packed row of the row sequence
+    long long seq;
+    int task, b, Lx, Ly, rows, ns, s;
+  };
+  auto make_item = [&](long long q, Item& it) {
+    it.seq = q;
+    it.s = 0;
     const long long tid = wg + q * nw;
     if (tid >= args.ntasks) {
-      t_ = -1; a_ = 0; b_ = 0; Lx_ = 1; Ly_ = 1; rows_ = 16; ns_ = 1;
+      it.task = -1; it.b = 0; it.Lx = 1; it.Ly = 1; it.rows = 16; it.ns = 1;
+      it.xb = args.xr;
       return;
     }
-    t_ = (int)tid;
+    it.task = (int)tid;
     int2 ab = decode_task((int)tid, args.mode, args.nY, args.list, args.order);
     if (ab.x < 0 || ab.x >= args.nX || ab.y < 0 || ab.y >= args.nYseq) {
       set_status(args.status, KSIG_ERR_INVALID);  // pair index out of range
       ab = make_int2(0, 0);
     }
-    a_ = ab.x; b_ = ab.y;
-    Lx_ = args.xlen[a_];
-    Ly_ = args.ylen[b_];
-    const int lx = DIFF ? Lx_ - 1 : Lx_;
-    const int ly = DIFF ? Ly_ - 1 : Ly_;
-    ns_ = ly <= STRIP ? 1 : (ly + STRIP - 1) / STRIP;
-    rows_ = lx > 16 ? lx : 16;
-    if (ns_ > 1 && rows_ < 32) rows_ = 32;
+    it.b = ab.y;
+    it.xb = args.xr + args.xstart[ab.x] * RS;
+    it.Lx = args.xlen[ab.x];
+    it.Ly = args.ylen[ab.y];
+    const int lx = DIFF ? it.Lx - 1 : it.Lx;
+    const int ly = DIFF ? it.Ly - 1 : it.Ly;
+    it.ns = ly <= STRIP ? 1 : (ly + STRIP - 1) / STRIP;
+    it.rows = lx > 16 ? lx : 16;
+    if (it.ns > 1 && it.rows < 32) it.rows = 32;
+  };
+  auto next_of = [&](const Item& cur, Item& nx) {
+    if (cur.task >= 0 && cur.s + 1 < cur.ns) {
+      nx = cur;
+      nx.s = cur.s + 1;
+    } else {
+      make_item(cur.seq + 1, nx);
+    }
+  };
+  auto ycol_ptr = [&](const Item& it, int c) {
+    int col = it.s * STRIP + C * lane + c;
+    col = col < it.Ly - 1 ? col : it.Ly - 1;
+    return args.yr + (args.ystart[it.b] + col) * RS;
+  };
+  // Stages the lane's column points of `it` into its smem slot.
+  auto stage_y = [&](const Item& it) {
+    if (it.task < 0) return;
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      const T* src = ycol_ptr(it, c);
+#pragma unroll
+      for (int v = 0; v < RS / VN; ++v)
+        __pipeline_memcpy_async(yslot + c * RS + v * VN, src + v * VN, 16);
+    }
+    __pipeline_commit();
   };
 
   T yv[C][KD + 1];
-  const T* xbase = args.xr;
-  int gLx = 1;
-
-  auto load_y = [&](int b_, int Ly_, int s_) {
-    const int g0 = s_ * STRIP + C * lane;
-    const T* ybase = args.yr + args.ystart[b_] * RS;
+  auto y_from_slot = [&]() {
+    __pipeline_wait_prior(0);
 #pragma unroll
     for (int c = 0; c < C; ++c) {
-      int col = g0 + c;
-      col = col < Ly_ - 1 ? col : Ly_ - 1;
-      const V* p = reinterpret_cast<const V*>(ybase + (long long)col * RS);
       T tmp[RS];
 #pragma unroll
-      for (int v = 0; v < RS / VN; ++v) reinterpret_cast<V*>(tmp)[v] = __ldg(p + v);
+      for (int v = 0; v < RS / VN; ++v)
+        reinterpret_cast<V*>(tmp)[v] = reinterpret_cast<const V*>(yslot + c * RS)[v];
 #pragma unroll
       for (int k = 0; k <= KD; ++k) yv[c][k] = tmp[k];
     }
   };
-
-  auto gram_row = [&](int row, T (&m)[C]) {
-    row = row < gLx - 1 ? row : gLx - 1;
-    const V* p = reinterpret_cast<const V*>(xbase + (long long)row * RS);
-    T xv[RS];
+  auto load_x = [&](const T* xb, int Lx, int row, T (&xv)[RS]) {
+    row = row < Lx - 1 ? row : Lx - 1;
+    const V* p = reinterpret_cast<const V*>(xb + (long long)row * RS);
 #pragma unroll
     for (int v = 0; v < RS / VN; ++v) reinterpret_cast<V*>(xv)[v] = __ldg(p + v);
+  };
+  auto gram = [&](const T (&xv)[RS], T (&m)[C]) {
 #pragma unroll
     for (int c = 0; c < C; ++c) {
       T acc = xv[KD] + yv[c][KD];
@@ -132,56 +170,103 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol) {
     }
   };
 
-  T Mcur[C], DMcur[C];
-  load_task(0, task, a, b, Lx, Ly, rows, ns);
-  xbase = args.xr + (task >= 0 ? args.xstart[a] : 0) * RS;
-  gLx = Lx;
-  if (task >= 0) {
-    load_y(b, Ly, 0);
+  Item cur, nxt;
+  make_item(0, cur);
+  next_of(cur, nxt);
+  // First item's columns straight into registers; the next item is staged.
+  if (cur.task >= 0) {
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      const V* p = reinterpret_cast<const V*>(ycol_ptr(cur, c));
+      T tmp[RS];
+#pragma unroll
+      for (int v = 0; v < RS / VN; ++v) reinterpret_cast<V*>(tmp)[v] = __ldg(p + v);
+#pragma unroll
+      for (int k = 0; k <= KD; ++k) yv[c][k] = tmp[k];
+    }
   } else {
 #pragma unroll
     for (int c = 0; c < C; ++c)
 #pragma unroll
       for (int k = 0; k <= KD; ++k) yv[c][k] = T(0);
   }
-  gram_row(0, Mcur);
+  stage_y(nxt);
+
+  T Mcur[C], DMcur[C];
+  T xv[RS];
+  load_x(cur.xb, cur.Lx, 0, xv);
+  gram(xv, Mcur);
 #pragma unroll
   for (int c = 0; c < C; ++c) DMcur[c] = T(0);
-  pol.begin_item();
-  if (task >= 0) pol.begin_task(ItemInfo{task, Lx, Ly, 0, ns}, lane);
+  load_x(cur.xb, cur.Lx, 1, xv);  // Gram row of the first step
 
+  // Cell work recorded at one step and executed at the next, so that a
+  // step's Gram and its cell recursion form one branch-free block the
+  // compiler can interleave.  `pit` is the item of the recorded row.
+  bool pv = false, plast = false;
+  int pr = 0;
+  Item pit = cur;
+  T pDM[C], pR = T(0);
+#pragma unroll
+  for (int c = 0; c < C; ++c) pDM[c] = T(0);
+
+  int u = 0;
   int delay = lane;
-  bool done = task < 0;
+  bool done = cur.task < 0;
   for (;;) {
-    if (__all_sync(FULL, done)) break;
+    if (__all_sync(FULL, done && !pv)) break;
     const bool active = delay == 0 && !done;
+    const bool last_row = (u == cur.rows);
 
-    // Exchange values of the same cell row from lane l-1 (one step earlier).
+    // ---- rare, uniform branches: item switches --------------------------
+    if (__any_sync(FULL, active && last_row)) {
+      if (active && last_row && nxt.task >= 0) y_from_slot();
+    }
+    if (__any_sync(FULL, pv && pr == 0)) {
+      if (pv && pr == 0) {
+        pol.begin_item();
+        if (pit.s == 0) pol.begin_task(ItemInfo{pit.task, pit.Lx, pit.Ly, pit.s, pit.ns}, lane);
+      }
+    }
+
+    // ---- main block: cells of the recorded row + Gram of the next row -----
     T Xin[NX];
 #pragma unroll
     for (int h = 0; h < NX; ++h) Xin[h] = shfl_up(pol.X[h], 1);
-
-    const bool last_row = (u == rows);
-    int ntask = task, na = a, nb = b, nLx = Lx, nLy = Ly, nrows = rows, nns = ns, ns_next = s;
-    long long nseq = seq;
-    if (__any_sync(FULL, active && last_row)) {
-      if (active && last_row) {
-        if (s + 1 < ns) {
-          ns_next = s + 1;
-        } else {
-          nseq = seq + 1;
-          load_task(nseq, ntask, na, nb, nLx, nLy, nrows, nns);
-          ns_next = 0;
-        }
-        if (ntask >= 0) {
-          xbase = args.xr + args.xstart[na] * RS;
-          gLx = nLx;
-          load_y(nb, nLy, ns_next);
-        }
+    if (lane == 0) {
+      if (pit.s > 0 && pv) {
+        const T* src = bbuf + (long long)pr * NX;
+#pragma unroll
+        for (int h = 0; h < NX; ++h) Xin[h] = __ldcg(src + h);
+      } else {
+        pol.left_boundary(Xin);
       }
     }
+    T Z[C];
+    if (DIFF) {
+#pragma unroll
+      for (int c = 0; c < C - 1; ++c) Z[c] = pDM[c + 1] - pDM[c];
+      Z[C - 1] = pR - pDM[C - 1];
+    } else {
+      const int g0 = pit.s * STRIP + C * lane;
+#pragma unroll
+      for (int c = 0; c < C; ++c)
+        Z[c] = (pr < pit.Lx && g0 + c < pit.Ly) ? pDM[c] : T(0);
+    }
+    // Lane 31's last cell belongs to the next strip when differencing.
+    const bool mask_last = DIFF && lane == 31;
+    if (mask_last) Z[C - 1] = T(0);
+#pragma unroll
+    for (int c = 0; c < C; ++c) Z[c] = pv ? Z[c] : T(0);
+    pol.row(Z, Xin, mask_last, pv, pr, ItemInfo{pit.task, pit.Lx, pit.Ly, pit.s, pit.ns}, lane);
+    if (lane == 31 && pv && pit.s + 1 < pit.ns) {
+      T* dst = bbuf + (long long)pr * NX;
+#pragma unroll
+      for (int h = 0; h < NX; ++h) __stcg(dst + h, pol.X[h]);
+    }
+
     T Mnew[C];
-    gram_row(last_row ? 0 : u + 1, Mnew);
+    gram(xv, Mnew);
     // With differencing DM holds vertical differences of grid rows; without
     // it DM carries the previous grid row (the cells of row u-1 themselves).
     T DMnew[C];
@@ -189,67 +274,55 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol) {
     for (int c = 0; c < C; ++c) DMnew[c] = DIFF ? Mnew[c] - Mcur[c] : Mcur[c];
     const T DMright = shfl_down(DMnew[0], 1);
 
-    if (active && u >= 1 && task >= 0) {
-      const int r = u - 1;
-      if (lane == 0) {
-        if (s > 0) {
-          const T* src = bbuf + (long long)r * NX;
-#pragma unroll
-          for (int h = 0; h < NX; ++h) Xin[h] = __ldcg(src + h);
-        } else {
-          pol.left_boundary(Xin);
+    // ---- end of a recorded item / pair (rare, uniform) --------------------
+    const bool fin_item = pv && plast;
+    bool fin = false;
+    if (__any_sync(FULL, fin_item)) {
+      if (fin_item) {
+        pol.end_item();
+        if (pit.s + 1 >= pit.ns) {
+          pol.end_task(pit.seq, pit.task, lane);
+          fin = true;
         }
-      }
-      T Z[C];
-      if (DIFF) {
-#pragma unroll
-        for (int c = 0; c < C - 1; ++c) Z[c] = DMcur[c + 1] - DMcur[c];
-        Z[C - 1] = DMright - DMcur[C - 1];
-      } else {
-        const int g0 = s * STRIP + C * lane;
-#pragma unroll
-        for (int c = 0; c < C; ++c)
-          Z[c] = (r < Lx && g0 + c < Ly) ? DMcur[c] : T(0);
-      }
-      // Lane 31's last cell belongs to the next strip when differencing.
-      const bool mask_last = DIFF && lane == 31;
-      if (mask_last) Z[C - 1] = T(0);
-      pol.row(Z, Xin, mask_last, r, ItemInfo{task, Lx, Ly, s, ns}, lane);
-      if (lane == 31 && s + 1 < ns) {
-        T* dst = bbuf + (long long)r * NX;
-#pragma unroll
-        for (int h = 0; h < NX; ++h) __stcg(dst + h, pol.X[h]);
       }
     }
     if (args.multi_strip) __syncwarp();
-
-    bool finished_task = false;
-    long long fin_seq = seq;
-    int fin_task = task;
-    if (active && last_row) {
-      if (s + 1 >= ns && task >= 0) {
-        finished_task = true;
-        pol.end_task(seq, task, lane);
-      }
-      pol.begin_item();
-      task = ntask; a = na; b = nb; Lx = nLx; Ly = nLy; rows = nrows; ns = nns;
-      if (nseq != seq && task >= 0) pol.begin_task(ItemInfo{task, Lx, Ly, 0, ns}, lane);
-      s = ns_next; seq = nseq; u = 0;
-      if (task < 0) done = true;
-    } else if (active) {
-      ++u;
+    // A pair is complete once lane 31 (the last lane) has finished it.
+    if (__shfl_sync(FULL, fin ? 1 : 0, 31)) {
+      const long long q = __shfl_sync(FULL, pit.seq, 31);
+      const int t = __shfl_sync(FULL, pit.task, 31);
+      pol.collect(q, t, lane);
     }
+
+    // ---- record cell row u-1 for the next step, advance ------------------
+    const bool rec = active && u >= 1 && cur.task >= 0;
+#pragma unroll
+    for (int c = 0; c < C; ++c) pDM[c] = rec ? DMcur[c] : pDM[c];
+    pR = rec ? DMright : pR;
+    pr = rec ? u - 1 : pr;
+    plast = rec && last_row;
+    pv = rec;
     if (active) {
 #pragma unroll
       for (int c = 0; c < C; ++c) { DMcur[c] = DMnew[c]; Mcur[c] = Mnew[c]; }
+      ++u;
     }
-
-    // A pair is complete once lane 31 (the last lane) has finished it.
-    const int l31_fin = __shfl_sync(FULL, finished_task ? 1 : 0, 31);
-    if (l31_fin) {
-      const long long q = __shfl_sync(FULL, fin_seq, 31);
-      const int t = __shfl_sync(FULL, fin_task, 31);
-      pol.collect(q, t, lane);
+    // Item switch of the position (rare, uniform).
+    if (__any_sync(FULL, (active && last_row) || (rec && u == 2))) {
+      if (rec && u == 2) pit = cur;          // first recorded row of cur
+      if (active && last_row) {
+        pit = cur;                           // last row recorded for cur
+        cur = nxt;
+        next_of(cur, nxt);
+        if (cur.task < 0) done = true;
+        else stage_y(nxt);
+        u = 0;
+      }
+    }
+    // Prefetch the x row of the next step's Gram.
+    {
+      const bool sw = (u == cur.rows);
+      load_x(sw ? nxt.xb : cur.xb, sw ? nxt.Lx : cur.Lx, sw ? 0 : u + 1, xv);
     }
     if (delay > 0) --delay;
   }
@@ -280,14 +353,18 @@ struct DpLayout {
 // sums live in Ccol (per lane, per column), the running sum over j' < j is
 // the exchange value H handed from lane to lane.  Row prefixes (axis -1) are
 // exchange values too; column prefixes (axis -2) are column sums.
+// Level totals need no extra work per cell: the column sum of sum R_k is
+// already kept for level k+1, so level k = sum_j Ccol at the end of a strip
+// (one more column sum for the last level).  Strip totals are reduced in
+// FP64.
 template <typename T, int C, int NL, int P, int WPB>
 struct DpPolicy {
   using L = DpLayout<NL, P>;
   static constexpr int NX = L::NH > 0 ? L::NH : 1;
   T X[NX];                    // horizontal running sums (outgoing)
   T Ccol[NX][C];              // column running sums
-  float accs[NL + 1], accc[NL + 1];
-  double accd[NL + 1];
+  T Clast[C];                 // column sums of the last level's totals
+  double accd[NL + 1];        // per-lane level totals of finished strips
   double (*red)[NL][32];      // this warp's [2][NL][32] reduction slots
   double* out;
   int ntasks, nl_out;
@@ -295,15 +372,17 @@ struct DpPolicy {
   __device__ void init(double (*red_)[NL][32], double* out_, int ntasks_, int nl_out_) {
     red = red_; out = out_; ntasks = ntasks_; nl_out = nl_out_;
 #pragma unroll
-    for (int k = 0; k <= NL; ++k) { accs[k] = 0.f; accc[k] = 0.f; accd[k] = 0.0; }
+    for (int k = 0; k <= NL; ++k) accd[k] = 0.0;
 #pragma unroll
     for (int h = 0; h < NX; ++h) X[h] = T(0);
   }
   __device__ void begin_item() {
 #pragma unroll
-    for (int h = 0; h < NX; ++h)
+    for (int c = 0; c < C; ++c) {
+      Clast[c] = T(0);
 #pragma unroll
-      for (int c = 0; c < C; ++c) Ccol[h][c] = T(0);
+      for (int h = 0; h < NX; ++h) Ccol[h][c] = T(0);
+    }
   }
   __device__ void begin_task(const ItemInfo&, int) {}
   __device__ void left_boundary(T (&Xin)[NX]) {
@@ -311,14 +390,13 @@ struct DpPolicy {
     for (int h = 0; h < NX; ++h) Xin[h] = T(0);
   }
 
-  __device__ void row(const T (&Z)[C], const T (&Xin)[NX], bool, int,
+  // Branch-free; with all Z = 0 (no recorded row) the state is unchanged
+  // apart from X, which no active neighbour reads then.
+  __device__ void row(const T (&Z)[C], const T (&Xin)[NX], bool, bool, int,
                       const ItemInfo&, int) {
     T H[NX];
 #pragma unroll
     for (int h = 0; h < NX; ++h) H[h] = Xin[h];
-    T rowacc[NL + 1];
-#pragma unroll
-    for (int k = 0; k <= NL; ++k) rowacc[k] = T(0);
 #pragma unroll
     for (int c = 0; c < C; ++c) {
       const T z = Z[c];
@@ -328,16 +406,10 @@ struct DpPolicy {
 #pragma unroll
         for (int j = 0; j < P; ++j) Rp[i][j] = T(0);
       Rp[0][0] = z;
-      rowacc[1] += z;
+      T tot = z;  // sum of the current level's states
 #pragma unroll
       for (int k = 2; k <= NL; ++k) {
         const int f = L::f(k), fp = L::f(k - 1), o = L::off(k);
-        T A = T(0);
-#pragma unroll
-        for (int i = 0; i < P; ++i)
-#pragma unroll
-          for (int j = 0; j < P; ++j)
-            if (i < fp && j < fp) A += Rp[i][j];
         T Rn[P][P];
 #pragma unroll
         for (int i = 0; i < P; ++i)
@@ -345,7 +417,7 @@ struct DpPolicy {
           for (int j = 0; j < P; ++j) Rn[i][j] = T(0);
         Rn[0][0] = z * H[o];
         H[o] += Ccol[o][c];
-        Ccol[o][c] += A;
+        Ccol[o][c] += tot;
         T lsum = Rn[0][0];
 #pragma unroll
         for (int rr = 1; rr < P; ++rr) {
@@ -369,40 +441,42 @@ struct DpPolicy {
             }
           }
         }
-        rowacc[k] += lsum;
+        tot = lsum;
 #pragma unroll
         for (int i = 0; i < P; ++i)
 #pragma unroll
           for (int j = 0; j < P; ++j) Rp[i][j] = Rn[i][j];
       }
+      Clast[c] += tot;
     }
 #pragma unroll
     for (int h = 0; h < NX; ++h) X[h] = H[h];
-    // Compensated (Neumaier) accumulation of the row partials.
+  }
+
+  // Folds a finished strip's column totals into the lane's level totals.
+  __device__ void end_item() {
 #pragma unroll
-    for (int k = 1; k <= NL; ++k) {
-      if (sizeof(T) == 8) {
-        accd[k] += (double)rowacc[k];
-      } else {
-        const float x = (float)rowacc[k];
-        const float t = accs[k] + x;
-        const float e = fabsf(accs[k]) >= fabsf(x) ? (accs[k] - t) + x : (x - t) + accs[k];
-        accc[k] += e;
-        accs[k] = t;
-      }
+    for (int k = 1; k < NL; ++k) {
+      double s = 0.0;
+#pragma unroll
+      for (int c = 0; c < C; ++c) s += (double)Ccol[L::off(k + 1)][c];
+      accd[k] += s;
     }
+    double s = 0.0;
+#pragma unroll
+    for (int c = 0; c < C; ++c) s += (double)Clast[c];
+    accd[NL] += s;
   }
 
   __device__ void end_task(long long seq, int, int lane) {
 #pragma unroll
     for (int k = 1; k <= NL; ++k) {
-      const double v = sizeof(T) == 8 ? accd[k] : (double)accs[k] + (double)accc[k];
-      red[seq & 1][k - 1][lane] = v;
-      accs[k] = 0.f; accc[k] = 0.f; accd[k] = 0.0;
+      red[seq & 1][k - 1][lane] = accd[k];
+      accd[k] = 0.0;
     }
   }
 
-  // Warp-wide: sum the 32 lanes' level sums of task t (FP64, fixed order).
+  // Warp-wide: sum the 32 lanes' level totals of task t (FP64, fixed order).
   __device__ void collect(long long q, int t, int lane) {
     __syncwarp();
 #pragma unroll
@@ -421,9 +495,11 @@ template <typename T, int KD, int C, int NL, int P, bool DIFF, int WPB>
 __global__ void __launch_bounds__(WPB * 32)
 dp_fwd_kernel(const SweepArgs<T> args) {
   __shared__ double red[WPB][2][NL][32];
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  auto* sm = reinterpret_cast<SweepSmem<T, KD, C>*>(dyn_smem);
   DpPolicy<T, C, NL, P, WPB> pol;
   pol.init(red[threadIdx.x >> 5], args.out, args.ntasks, args.nl_out);
-  sweep<T, KD, C, DIFF, WPB>(args, pol);
+  sweep<T, KD, C, DIFF, WPB>(args, pol, sm[threadIdx.x >> 5]);
 }
 
 // ---------------------------------------------------------------------------
@@ -483,8 +559,9 @@ struct PdePolicy {
     for (int f = 0; f < F; ++f) { Xin[f] = T(1); Xin[F + f] = T(0); }
   }
 
-  __device__ void row(const T (&Z)[C], const T (&Xin)[NX], bool mask_last, int r,
-                      const ItemInfo& it, int lane) {
+  __device__ void row(const T (&Z)[C], const T (&Xin)[NX], bool mask_last, bool valid,
+                      int r, const ItemInfo& it, int lane) {
+    if (!valid) return;
     T a[C], b[C];
     constexpr T inv = T(1) / T(F * F);
 #pragma unroll
@@ -529,6 +606,7 @@ struct PdePolicy {
       out[it.task] = (double)captured;
     }
   }
+  __device__ void end_item() {}
   __device__ void end_task(long long, int, int) {}
   __device__ void collect(long long, int, int) {}
 };
@@ -536,9 +614,11 @@ struct PdePolicy {
 template <typename T, int KD, int C, int F, bool DIFF, int WPB>
 __global__ void __launch_bounds__(WPB * 32)
 pde_fwd_kernel(const SweepArgs<T> args) {
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  auto* sm = reinterpret_cast<SweepSmem<T, KD, C>*>(dyn_smem);
   PdePolicy<T, C, F, DIFF> pol;
   pol.init(args.out);
-  sweep<T, KD, C, DIFF, WPB>(args, pol);
+  sweep<T, KD, C, DIFF, WPB>(args, pol, sm[threadIdx.x >> 5]);
 }
 
 }  // namespace ksig

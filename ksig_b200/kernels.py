@@ -26,6 +26,7 @@ from typing import Optional
 import numpy as np
 import torch
 
+from . import _autograd as AG
 from . import _engine as E
 from . import _lib as L
 from . import static as static_mod
@@ -138,12 +139,34 @@ class SignatureBase:
       return K
     return K.detach().cpu().numpy()
 
-  def _param_requires_grad(self):
-    p = getattr(self.static_kernel, 'bandwidth', None)
-    return isinstance(p, torch.Tensor) and p.requires_grad
+  def _param_tensor(self):
+    sk = self.static_kernel
+    p = getattr(sk, 'bandwidth', None)
+    if p is None:
+      p = getattr(sk, 'scale', None)
+    return p if isinstance(p, torch.Tensor) else None
 
-  def _K_autograd(self, *args):
-    raise NotImplementedError('gradients are not available for this kernel')
+  def _param_requires_grad(self):
+    p = self._param_tensor()
+    return p is not None and p.requires_grad
+
+  def _levels_bwd(self, Xs, Ys, mode, grad_levels, want_dparam):
+    raise NotImplementedError(
+        f'gradients are not available for {type(self).__name__}')
+
+  def _K_autograd(self, Xin, Xs, gx, Ys, gy, sym):
+    """Differentiable K(X, Y) / K(X) through the hand-written adjoint."""
+    kind, param = self._static()
+    pt = self._param_tensor()
+    spec = dict(Xs=Xs, Ys=Ys, normalize=self.normalize, kind=kind,
+                param=float(param), levels_fn=self._levels,
+                bwd_fn=self._levels_bwd,
+                param_dtype=pt.dtype if pt is not None else torch.float64,
+                param_device=pt.device if pt is not None else 'cpu')
+    if sym:
+      gy = None
+    return AG.SigKernelFn.apply(gx, gy, pt if (pt is not None and pt.requires_grad)
+                                else None, spec)
 
 
 class SignatureKernel(SignatureBase):
@@ -162,6 +185,11 @@ class SignatureKernel(SignatureBase):
     kind, param = self._static()
     return E.sig_levels(Xs, Ys, mode, self.n_levels, self.order,
                         self.difference, kind, param)
+
+  def _levels_bwd(self, Xs, Ys, mode, grad_levels, want_dparam):
+    kind, param = self._static()
+    return E.sig_levels_bwd(Xs, Ys, mode, self.n_levels, self.order, kind,
+                            param, grad_levels, want_dparam=want_dparam)
 
   def _Kdiag(self, Xs):
     """ksig/kernels.py:166-178: ones when normalising."""
@@ -212,3 +240,8 @@ class SignaturePDEKernel(SignatureKernel):
     v = E.pde_values(Xs, Ys, mode, self.dyadic_order, self.difference, kind,
                      param)
     return v[None, :]
+
+  def _levels_bwd(self, Xs, Ys, mode, grad_levels, want_dparam):
+    kind, param = self._static()
+    return E.pde_values_bwd(Xs, Ys, mode, self.dyadic_order, kind, param,
+                            grad_levels[0], want_dparam=want_dparam)

@@ -1,0 +1,103 @@
+"""Gradients of the CUDA adjoint against autograd through the FP64 torch
+oracle (itself pinned to central finite differences in
+tests/test_oracle_grad.py).  Tolerance: 1e-4 relative for FP32 inputs (the
+north-star bar for gradients), 1e-8 for FP64 inputs."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import ksig_oracle_torch as OT
+
+pytestmark = pytest.mark.gpu
+
+
+def _walks(rng, n, L, d, scale=0.3):
+  return np.cumsum(rng.standard_normal((n, L, d)) * scale, axis=1)
+
+
+def _relerr(a, b):
+  a = a.detach().cpu().double().numpy()
+  b = b.detach().cpu().double().numpy()
+  return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def _run(kern_factory, oracle_fn, X, Y, bw, dt, tol, sym=False):
+  import ksig_b200 as K
+  w_rng = np.random.default_rng(123)
+  # ours
+  Xt = torch.tensor(X, dtype=dt, device='cuda', requires_grad=True)
+  Yt = None if sym else torch.tensor(Y, dtype=dt, device='cuda', requires_grad=True)
+  bt = torch.tensor(bw, dtype=torch.float64, requires_grad=True)
+  kern = kern_factory(K, bt)
+  out = kern(Xt) if sym else kern(Xt, Yt)
+  W = torch.tensor(w_rng.standard_normal(tuple(out.shape)), device='cuda',
+                   dtype=out.dtype)
+  (out * W).sum().backward()
+  # oracle on the same (rounded) inputs
+  Xo = [torch.tensor(x, dtype=torch.float64, requires_grad=True)
+        for x in Xt.detach().double().cpu().numpy()]
+  Yo = None if sym else [torch.tensor(y, dtype=torch.float64, requires_grad=True)
+                         for y in Yt.detach().double().cpu().numpy()]
+  bo = torch.tensor(bw, dtype=torch.float64, requires_grad=True)
+  ref = oracle_fn(Xo, Yo, bo)
+  assert _relerr(out, ref) < tol
+  (ref * W.double().cpu()).sum().backward()
+  gX = torch.stack([x.grad for x in Xo])
+  assert _relerr(Xt.grad, gX) < tol, ('dX', _relerr(Xt.grad, gX))
+  if not sym:
+    gY = torch.stack([y.grad for y in Yo])
+    assert _relerr(Yt.grad, gY) < tol, ('dY', _relerr(Yt.grad, gY))
+  assert abs(bt.grad.item() - bo.grad.item()) <= tol * max(1.0, abs(bo.grad.item())), \
+      ('dbw', bt.grad.item(), bo.grad.item())
+
+
+@pytest.mark.parametrize('dt,tol', [(torch.float64, 1e-8), (torch.float32, 1e-4)])
+@pytest.mark.parametrize('normalize', [True, False])
+@pytest.mark.parametrize('order,n_levels', [(1, 4), (2, 4), (3, 5)])
+def test_dp_grad_rect(dt, tol, normalize, order, n_levels):
+  rng = np.random.default_rng(order * 7 + n_levels)
+  X = _walks(rng, 3, 23, 3)
+  Y = _walks(rng, 2, 17, 3)
+  _run(lambda K, b: K.SignatureKernel(n_levels=n_levels, order=order,
+                                      normalize=normalize,
+                                      static_kernel=K.RBFKernel(b)),
+       lambda x, y, b: OT.signature_kernel(x, y, n_levels=n_levels,
+                                           order=order, normalize=normalize,
+                                           param=b),
+       X, Y, 0.8, dt, tol)
+
+
+@pytest.mark.parametrize('dt,tol', [(torch.float64, 1e-8), (torch.float32, 1e-4)])
+@pytest.mark.parametrize('normalize', [True, False])
+def test_dp_grad_sym(dt, tol, normalize):
+  rng = np.random.default_rng(5)
+  X = _walks(rng, 4, 19, 2)
+  _run(lambda K, b: K.SignatureKernel(n_levels=5, order=1, normalize=normalize,
+                                      static_kernel=K.RBFKernel(b)),
+       lambda x, y, b: OT.signature_kernel(x, None, n_levels=5, order=1,
+                                           normalize=normalize, param=b),
+       X, None, 0.7, dt, tol, sym=True)
+
+
+def test_dp_grad_linear_fp64():
+  rng = np.random.default_rng(8)
+  X = _walks(rng, 2, 15, 3)
+  Y = _walks(rng, 3, 12, 3)
+  _run(lambda K, b: K.SignatureKernel(n_levels=4, order=2, normalize=True,
+                                      static_kernel=K.LinearKernel(b)),
+       lambda x, y, b: OT.signature_kernel(x, y, n_levels=4, order=2,
+                                           normalize=True, kind='linear',
+                                           param=b),
+       X, Y, 0.6, torch.float64, 1e-8)
+
+
+@pytest.mark.parametrize('L', [140, 300])
+def test_dp_grad_multi_strip_fp64(L):
+  rng = np.random.default_rng(L)
+  X = _walks(rng, 2, L, 2, scale=0.1)
+  Y = _walks(rng, 1, L - 9, 2, scale=0.1)
+  _run(lambda K, b: K.SignatureKernel(n_levels=3, order=2, normalize=True,
+                                      static_kernel=K.RBFKernel(b)),
+       lambda x, y, b: OT.signature_kernel(x, y, n_levels=3, order=2,
+                                           normalize=True, param=b),
+       X, Y, 0.9, torch.float64, 1e-8)
