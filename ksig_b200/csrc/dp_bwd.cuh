@@ -484,6 +484,10 @@ dp_bwd_kernel(const DpBwdArgs<T> args) {
           }
           T Rb_next[C][P][P];
           T Ub[P];
+          // Column-suffix increments of the level processed last: they are
+          // added to DA only after the next lower level has read DA, so that
+          // every suffix used in row r covers rows > r only.
+          T pendDA[P][C];
 #pragma unroll
           for (int c = 0; c < C; ++c) Zb[c] = T(0);
 #pragma unroll
@@ -555,15 +559,21 @@ dp_bwd_kernel(const DpBwdArgs<T> args) {
 #pragma unroll
                 for (int j = 0; j < P; ++j) Rb_next[c][i][j] = Rb[i][j];
             }
-            // Column suffix sums now include row r for the rows above.
+            // Level k+1's increments can go in now that level k has used DA.
+            if (k < NL) {
+#pragma unroll
+              for (int c = 0; c < C; ++c)
+#pragma unroll
+                for (int rr = 0; rr < P; ++rr)
+                  if (rr < fn) DA[on + rr][c] += pendDA[rr][c];
+            }
             if (k >= 2) {
-              const int o = Lay::off(k);
 #pragma unroll
               for (int c = 0; c < C; ++c) {
-                DA[o][c] += Z[c] * Rb_next[c][0][0];
+                pendDA[0][c] = Z[c] * Rb_next[c][0][0];
 #pragma unroll
                 for (int rr = 1; rr < P; ++rr)
-                  if (rr < f) DA[o + rr][c] += Z[c] * (T(1) / T(rr + 1)) * Rb_next[c][0][rr];
+                  pendDA[rr][c] = (rr < f) ? Z[c] * (T(1) / T(rr + 1)) * Rb_next[c][0][rr] : T(0);
               }
             }
           }

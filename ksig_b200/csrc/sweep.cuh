@@ -213,28 +213,15 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
   int u = 0;
   int delay = lane;
   bool done = cur.task < 0;
-  for (;;) {
-    if (__all_sync(FULL, done && !pv)) break;
-    const bool active = delay == 0 && !done;
-    const bool last_row = (u == cur.rows);
 
-    // ---- rare, uniform branches: item switches --------------------------
-    if (__any_sync(FULL, active && last_row)) {
-      if (active && last_row && nxt.task >= 0) y_from_slot();
-    }
-    if (__any_sync(FULL, pv && pr == 0)) {
-      if (pv && pr == 0) {
-        pol.begin_item();
-        if (pit.s == 0) pol.begin_task(ItemInfo{pit.task, pit.Lx, pit.Ly, pit.s, pit.ns}, lane);
-      }
-    }
-
-    // ---- main block: cells of the recorded row + Gram of the next row -----
+  // Cells of the recorded row + Gram of the next grid row.  `pvf` is false
+  // only when nothing was recorded (Z is forced to zero then).
+  auto main_block = [&](bool pvf, T (&Mnew)[C], T (&DMnew)[C], T& DMright) {
     T Xin[NX];
 #pragma unroll
     for (int h = 0; h < NX; ++h) Xin[h] = shfl_up(pol.X[h], 1);
     if (lane == 0) {
-      if (pit.s > 0 && pv) {
+      if (pit.s > 0 && pvf) {
         const T* src = bbuf + (long long)pr * NX;
 #pragma unroll
         for (int h = 0; h < NX; ++h) Xin[h] = __ldcg(src + h);
@@ -256,25 +243,69 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
     // Lane 31's last cell belongs to the next strip when differencing.
     const bool mask_last = DIFF && lane == 31;
     if (mask_last) Z[C - 1] = T(0);
-#pragma unroll
-    for (int c = 0; c < C; ++c) Z[c] = pv ? Z[c] : T(0);
-    pol.row(Z, Xin, mask_last, pv, pr, ItemInfo{pit.task, pit.Lx, pit.Ly, pit.s, pit.ns}, lane);
-    if (lane == 31 && pv && pit.s + 1 < pit.ns) {
+    pol.row(Z, Xin, mask_last, pvf, pr, ItemInfo{pit.task, pit.Lx, pit.Ly, pit.s, pit.ns}, lane);
+    if (lane == 31 && pvf && pit.s + 1 < pit.ns) {
       T* dst = bbuf + (long long)pr * NX;
 #pragma unroll
       for (int h = 0; h < NX; ++h) __stcg(dst + h, pol.X[h]);
     }
-
-    T Mnew[C];
     gram(xv, Mnew);
     // With differencing DM holds vertical differences of grid rows; without
     // it DM carries the previous grid row (the cells of row u-1 themselves).
-    T DMnew[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) DMnew[c] = DIFF ? Mnew[c] - Mcur[c] : Mcur[c];
-    const T DMright = shfl_down(DMnew[0], 1);
+    DMright = shfl_down(DMnew[0], 1);
+    if (args.multi_strip) __syncwarp();
+  };
 
-    // ---- end of a recorded item / pair (rare, uniform) --------------------
+  for (;;) {
+    if (__all_sync(FULL, done && !pv)) break;
+
+    // ---- steady run: steps without any item event in any lane ----------
+    // A step is plain for a lane when it is active, its recorded row is not
+    // the first of an item (pr >= 1, i.e. u >= 3) and it is not the item's
+    // last step (u < rows); then no item switch, no begin/end hook and no
+    // pair completion happens, and every lane has a recorded row.
+    {
+      const bool plain = delay == 0 && !done && u >= 3 && u < cur.rows;
+      const int nplain = __reduce_min_sync(FULL, plain ? cur.rows - u : 0);
+      for (int it = 0; it < nplain; ++it) {
+        T Mnew[C], DMnew[C], DMright;
+        main_block(true, Mnew, DMnew, DMright);
+#pragma unroll
+        for (int c = 0; c < C; ++c) { pDM[c] = DMcur[c]; DMcur[c] = DMnew[c]; Mcur[c] = Mnew[c]; }
+        pR = DMright;
+        pr = u - 1;
+        ++u;
+        const bool sw = (u == cur.rows);
+        load_x(sw ? nxt.xb : cur.xb, sw ? nxt.Lx : cur.Lx, sw ? 0 : u + 1, xv);
+      }
+      if (nplain > 0) continue;
+    }
+
+    // ---- general step ----------------------------------------------------
+    const bool active = delay == 0 && !done;
+    const bool last_row = (u == cur.rows);
+
+    // Rare, uniform branches: item switches.
+    if (__any_sync(FULL, active && last_row)) {
+      if (active && last_row && nxt.task >= 0) y_from_slot();
+    }
+    if (__any_sync(FULL, pv && pr == 0)) {
+      if (pv && pr == 0) {
+        pol.begin_item();
+        if (pit.s == 0) pol.begin_task(ItemInfo{pit.task, pit.Lx, pit.Ly, pit.s, pit.ns}, lane);
+      }
+    }
+
+    // Zero the recorded differences when nothing was recorded, so Z = 0.
+#pragma unroll
+    for (int c = 0; c < C; ++c) pDM[c] = pv ? pDM[c] : T(0);
+    pR = pv ? pR : T(0);
+    T Mnew[C], DMnew[C], DMright;
+    main_block(pv, Mnew, DMnew, DMright);
+
+    // End of a recorded item / pair (rare, uniform).
     const bool fin_item = pv && plast;
     bool fin = false;
     if (__any_sync(FULL, fin_item)) {
@@ -285,16 +316,15 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
           fin = true;
         }
       }
-    }
-    if (args.multi_strip) __syncwarp();
-    // A pair is complete once lane 31 (the last lane) has finished it.
-    if (__shfl_sync(FULL, fin ? 1 : 0, 31)) {
-      const long long q = __shfl_sync(FULL, pit.seq, 31);
-      const int t = __shfl_sync(FULL, pit.task, 31);
-      pol.collect(q, t, lane);
+      // A pair is complete once lane 31 (the last lane) has finished it.
+      if (__shfl_sync(FULL, fin ? 1 : 0, 31)) {
+        const long long q = __shfl_sync(FULL, pit.seq, 31);
+        const int t = __shfl_sync(FULL, pit.task, 31);
+        pol.collect(q, t, lane);
+      }
     }
 
-    // ---- record cell row u-1 for the next step, advance ------------------
+    // Record cell row u-1 for the next step, advance.
     const bool rec = active && u >= 1 && cur.task >= 0;
 #pragma unroll
     for (int c = 0; c < C; ++c) pDM[c] = rec ? DMcur[c] : pDM[c];

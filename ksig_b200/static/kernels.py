@@ -62,7 +62,8 @@ class LinearKernel(StaticKernel):
 
   @property
   def param(self):
-    return float(self.scale)
+    v = self.scale
+    return float(v.detach()) if hasattr(v, 'detach') else float(v)
 
   def _K(self, X, Y=None):
     Y = X if Y is None else Y
@@ -80,7 +81,8 @@ class StationaryKernel(StaticKernel):
 
   @property
   def param(self):
-    return float(self.bandwidth)
+    v = self.bandwidth
+    return float(v.detach()) if hasattr(v, 'detach') else float(v)
 
   def _Kdiag(self, X):
     return torch.ones((X.shape[0],), dtype=X.dtype, device=X.device)
