@@ -157,6 +157,32 @@ int ksig_signature_kern_bwd(const void* X, const int32_t* lenX, int nX,
                             double* dparam, void* workspace,
                             size_t workspace_bytes, void* stream);
 
+/* Workspace (bytes) required by ksig_signature_kern_pde_bwd. */
+size_t ksig_signature_kern_pde_bwd_workspace(int nX, int LX, int nY, int LY,
+                                             int d, int dtype,
+                                             int dyadic_order, int difference,
+                                             int pairs_mode, int n_list);
+
+/*
+ * Adjoint of ksig_signature_kern_pde (no reference counterpart).  For every
+ * pair p = (a, b) and grad[p] = dL/dK(p) (float64 [P]) it accumulates
+ *   dX[a]   += grad[p] * dK(x_a, y_b) / d x_a   (row side only)
+ *   *dparam += grad[p] * dK(x_a, y_b) / d param
+ * with the exact discrete adjoint of the Goursat scheme at the given dyadic
+ * order.  dX has X's dtype and shape [nX, LX, d] and is not cleared; dparam
+ * may be NULL.  difference must be 1.  The workspace holds one refined
+ * adjoint grid per resident warp (a few GB at most for long sequences).
+ */
+int ksig_signature_kern_pde_bwd(const void* X, const int32_t* lenX, int nX,
+                                int LX, const void* Y, const int32_t* lenY,
+                                int nY, int LY, int d, int dtype,
+                                int static_kind, double static_param,
+                                int dyadic_order, int difference,
+                                int pairs_mode, const int32_t* pair_list,
+                                int n_list, const double* grad, void* dX,
+                                double* dparam, void* workspace,
+                                size_t workspace_bytes, void* stream);
+
 /*
  * Normalisation and level mean (replaces ksig/kernels.py:190-214).
  *   levels   float64 [n_lev, P] from one of the calls above with pairs_mode

@@ -93,7 +93,8 @@ class SigKernelFn(torch.autograd.Function):
     else:
       gK = G[None].expand(n_lev, nX, nY).clone()
       gKx = gKy = None
-    gK[0] = 0.0  # level 0 is the constant 1
+    if spec.get('const_level0', True):
+      gK[0] = 0.0  # DP level 0 is the constant 1
     want_x = ctx.needs_input_grad[0]
     want_y = ctx.needs_input_grad[1]
     want_p = ctx.needs_input_grad[2]

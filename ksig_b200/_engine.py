@@ -165,5 +165,26 @@ def np_dtype(t):
 
 def pde_values_bwd(X, Y, mode, dyadic_order, kind, param, grad, dX=None,
                    want_dparam=True, pair_list=None):
-  """Row-side adjoint of :func:`pde_values` (see ksig_signature_kern_pde_bwd)."""
-  raise NotImplementedError('the PDE adjoint is not built into this library')
+  """Row-side adjoint of :func:`pde_values`; returns ``(dX, dparam)``."""
+  lib = L.lib()
+  Yv = X if Y is None else Y
+  dt = _dtype_code(X.data)
+  n_list = 0 if pair_list is None else pair_list.shape[0]
+  if dX is None:
+    dX = torch.zeros_like(X.data)
+  dpar = torch.zeros((1,), dtype=torch.float64, device=X.data.device) \
+      if want_dparam else None
+  g = grad.to(torch.float64).contiguous()
+  ws_bytes = lib.ksig_signature_kern_pde_bwd_workspace(
+      X.n, X.L, Yv.n, Yv.L, X.d, dt, dyadic_order, 1, mode, n_list)
+  if ws_bytes == 0:
+    L.check(L.ERR_UNSUPPORTED if 'no compiled' in L.last_error()
+            else L.ERR_INVALID)
+  ws = _workspace(ws_bytes, X.data.device)
+  rc = lib.ksig_signature_kern_pde_bwd(
+      _ptr(X.data), _ptr(X.lengths), X.n, X.L, _ptr(Yv.data),
+      _ptr(Yv.lengths), Yv.n, Yv.L, X.d, dt, kind, float(param),
+      dyadic_order, 1, mode, _ptr(pair_list), n_list, _ptr(g), _ptr(dX),
+      _ptr(dpar), _ptr(ws), ws_bytes, _stream())
+  L.check(rc)
+  return dX, dpar

@@ -68,6 +68,11 @@ def instances():
   for dt in ('f32', 'f64'):
     for f, kd in itertools.product([1, 2, 4], KD_FEW):
       add(('pde', dt, kd, 2, 0, f, 0))
+  # PDE backward (row-side gradients).
+  for f, kd, c in itertools.product([1, 2, 4, 8], KD_ALL, [2, 4, 8]):
+    add(('pdeb', 'f32', kd, c, 0, f, 1))
+  for f, kd in itertools.product([1, 2, 4, 8], KD_FEW):
+    add(('pdeb', 'f64', kd, 2, 0, f, 1))
   # DP backward (row-side gradients).
   for dt, cs in (('f32', [2, 4]), ('f64', [2])):
     for nl, kd, c in itertools.product(NL_ALL, KD_ALL, cs):
@@ -84,6 +89,7 @@ OPS = {
     'dp': ('OP_DP_FWD', 'dp_fwd_kernel<{T}, {kd}, {c}, {nl}, {p}, {diff}, {wpb}>'),
     'pde': ('OP_PDE_FWD', 'pde_fwd_kernel<{T}, {kd}, {c}, {p}, {diff}, {wpb}>'),
     'dpb': ('OP_DP_BWD', 'dp_bwd_kernel<{T}, {kd}, {c}, {nl}, {p}, {wpb}>'),
+    'pdeb': ('OP_PDE_BWD', 'pde_bwd_kernel<{T}, {kd}, {c}, {p}, {wpb}>'),
 }
 
 
@@ -103,6 +109,7 @@ def generate():
   for key, insts in sorted(groups.items()):
     lines = ['// Generated by ksig_b200/build.py; do not edit.',
              '#include "../sweep.cuh"', '#include "../dp_bwd.cuh"',
+             '#include "../pde_bwd.cuh"',
              '#include "../registry.h"',
              'namespace ksig {']
     ents = []

@@ -16,6 +16,7 @@
 #include "registry.h"
 #include "sweep.cuh"
 #include "dp_bwd.cuh"
+#include "pde_bwd.cuh"
 
 namespace ksig {
 namespace {
@@ -432,6 +433,104 @@ int run_bwd(const BwdPlan& bp, const void* X, const int32_t* lenX, int nX, int L
   return KSIG_OK;
 }
 
+// PDE backward: the forward's packing layout plus, per warp, the reversed
+// adjoint grid G (refined rows x refined columns) and a strip boundary
+// buffer (pde_bwd.cuh).
+struct PdeBwdPlan {
+  FwdPlan f;
+  const KernelEntry* k;
+  int c, F, grid, rows_max;
+  long long grid_stride, bb_off, scratch_per_warp;
+  size_t off_scratch, total;
+};
+
+int plan_pde_bwd(int nX, int LX, int nY, int LY, int d, int dtype, int dyadic, int difference,
+                 int pairs_mode, int n_list, PdeBwdPlan& bp) {
+  int rc = plan_fwd(true, nX, LX, nY, LY, d, dtype, 0, dyadic, difference, pairs_mode, n_list,
+                    bp.f);
+  if (rc) return rc;
+  if (!difference) return fail(KSIG_ERR_UNSUPPORTED, "gradients need difference=True");
+  if (pairs_mode == KSIG_PAIRS_UPPER || pairs_mode == KSIG_PAIRS_DIAG) { nY = nX; LY = LX; }
+  const int ly = LY - 1, lx = LX - 1;
+  bp.F = 1 << dyadic;
+  const int forced = env_int("KSIG_BWD_COLS", 0);
+  const int want = forced > 0 ? forced : (ly <= 63 ? 2 : (ly <= 127 ? 4 : 8));
+  const KernelEntry* k = find_kernel(OP_PDE_BWD, bp.f.f64, d, want, 0, bp.F, 1);
+  if (!k)
+    return fail(KSIG_ERR_UNSUPPORTED, "no compiled PDE backward kernel for dtype=%s d=%d "
+                "dyadic_order=%d", bp.f.f64 ? "f64" : "f32", d, dyadic);
+  bp.k = k;
+  bp.c = k->c;
+  bp.rows_max = lx > 1 ? lx : 1;
+  const long long Nref = (long long)(lx > 1 ? lx : 1) * bp.F;
+  const long long Mref = (long long)(ly > 1 ? ly : 1) * bp.F;
+  bp.grid_stride = (Mref + 3) / 4 * 4;
+  bp.bb_off = Nref * bp.grid_stride;
+  bp.scratch_per_warp = bp.bb_off + (long long)bp.rows_max * (2 * bp.F + 2);
+  const size_t es = bp.f.f64 ? 8 : 4;
+  int occ = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k->func, k->wpb * 32, 0);
+  if (e != cudaSuccess || occ <= 0) occ = 1;
+  const int sms = sm_count() > 0 ? sm_count() : 148;
+  long long warps = (long long)sms * occ * k->wpb;
+  // Keep the adjoint grids within a few GB of scratch.
+  const long long budget = (long long)env_int("KSIG_PDE_BWD_SCRATCH_MB", 4096) << 20;
+  const long long cap = budget / (long long)(bp.scratch_per_warp * es);
+  if (warps > cap) warps = cap > (long long)k->wpb ? cap : k->wpb;
+  if (warps > bp.f.ntasks) warps = bp.f.ntasks > 0 ? bp.f.ntasks : 1;
+  bp.grid = (int)((warps + k->wpb - 1) / k->wpb);
+  bp.off_scratch = bp.f.off_scratch;
+  bp.total = align_up(bp.off_scratch + (size_t)bp.grid * k->wpb * bp.scratch_per_warp * es);
+  if (bp.total < bp.f.total) bp.total = bp.f.total;
+  return KSIG_OK;
+}
+
+template <typename T>
+int run_pde_bwd(const PdeBwdPlan& bp, const void* X, const int32_t* lenX, int nX, int LX,
+                const void* Y, const int32_t* lenY, int nY, int LY, int d, int src_f64,
+                int kind, double param, int mode, const int32_t* list, const double* grad,
+                void* dX, double* dparam, char* ws, cudaStream_t st) {
+  const FwdPlan& pl = bp.f;
+  int* status = reinterpret_cast<int*>(ws + pl.off_status);
+  T* xr = reinterpret_cast<T*>(ws + pl.off_xr);
+  T* yr = reinterpret_cast<T*>(ws + pl.off_yr);
+  int64_t* xs = reinterpret_cast<int64_t*>(ws + pl.off_xstart);
+  int64_t* ys = reinterpret_cast<int64_t*>(ws + pl.off_ystart);
+  int32_t* xl = reinterpret_cast<int32_t*>(ws + pl.off_xlen);
+  int32_t* yl = reinterpret_cast<int32_t*>(ws + pl.off_ylen);
+  const bool self = mode == KSIG_PAIRS_UPPER || mode == KSIG_PAIRS_DIAG;
+  int rc = pack<T>(X, lenX, nX, LX, d, src_f64, kind, param, 1, pl, xr, xs, xl, status, st);
+  if (rc) return rc;
+  if (self) rc = pack<T>(X, lenX, nX, LX, d, src_f64, kind, param, 0, pl, yr, ys, yl, status, st);
+  else rc = pack<T>(Y, lenY, nY, LY, d, src_f64, kind, param, 0, pl, yr, ys, yl, status, st);
+  if (rc) return rc;
+  PdeBwdArgs<T> a{};
+  a.xr = xr; a.xstart = xs; a.xlen = xl;
+  a.yr = yr; a.ystart = ys; a.ylen = yl;
+  a.mode = mode;
+  a.nY = self ? nX : nY;
+  a.list = reinterpret_cast<const int2*>(list);
+  a.ntasks = (int)pl.ntasks;
+  a.nX = nX;
+  a.nYseq = self ? nX : nY;
+  a.kind = kind;
+  a.param = param;
+  a.grad = grad;
+  a.dX = reinterpret_cast<T*>(dX);
+  a.LX = LX;
+  a.d = d;
+  a.dparam = dparam;
+  a.scratch = reinterpret_cast<T*>(ws + bp.off_scratch);
+  a.scratch_per_warp = bp.scratch_per_warp;
+  a.grid_stride = bp.grid_stride;
+  a.bb_off = bp.bb_off;
+  a.rows_max = bp.rows_max;
+  a.status = status;
+  void* kargs[] = {&a};
+  KSIG_CUDA(launch_main(bp.k->func, dim3(bp.grid), dim3(bp.k->wpb * 32), kargs, 0, st));
+  return KSIG_OK;
+}
+
 int check_common(const void* X, const void* Y, int pairs_mode, const int32_t* list, int n_list,
                  int static_kind, double static_param) {
   if (!X) return fail(KSIG_ERR_INVALID, "X is NULL");
@@ -586,6 +685,44 @@ int ksig_signature_kern_bwd(const void* X, const int32_t* lenX, int nX, int LX, 
   return run_bwd<float>(bp, X, lenX, nX, LX, Y, lenY, nY, LY, d, 0, static_kind, static_param,
                         pairs_mode, pair_list, grad_levels, n_levels, dX, dparam,
                         static_cast<char*>(workspace), st);
+}
+
+size_t ksig_signature_kern_pde_bwd_workspace(int nX, int LX, int nY, int LY, int d, int dtype,
+                                             int dyadic_order, int difference, int pairs_mode,
+                                             int n_list) {
+  PdeBwdPlan bp;
+  if (plan_pde_bwd(nX, LX, nY, LY, d, dtype, dyadic_order, difference, pairs_mode, n_list, bp))
+    return 0;
+  return bp.total;
+}
+
+int ksig_signature_kern_pde_bwd(const void* X, const int32_t* lenX, int nX, int LX,
+                                const void* Y, const int32_t* lenY, int nY, int LY, int d,
+                                int dtype, int static_kind, double static_param,
+                                int dyadic_order, int difference, int pairs_mode,
+                                const int32_t* pair_list, int n_list, const double* grad,
+                                void* dX, double* dparam, void* workspace,
+                                size_t workspace_bytes, void* stream) {
+  int rc = check_common(X, Y, pairs_mode, pair_list, n_list, static_kind, static_param);
+  if (rc) return rc;
+  if (!grad || !dX) return fail(KSIG_ERR_INVALID, "grad / dX is NULL");
+  PdeBwdPlan bp;
+  rc = plan_pde_bwd(nX, LX, nY, LY, d, dtype, dyadic_order, difference, pairs_mode, n_list, bp);
+  if (rc) return rc;
+  if (!workspace || workspace_bytes < bp.total)
+    return fail(KSIG_ERR_WORKSPACE, "workspace of %zu bytes is smaller than the %zu required",
+                workspace_bytes, bp.total);
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  KSIG_CUDA(cudaMemsetAsync(workspace, 0, 16, st));
+  if (bp.f.ntasks == 0) return KSIG_OK;
+  if (pairs_mode == KSIG_PAIRS_UPPER || pairs_mode == KSIG_PAIRS_DIAG) { nY = nX; LY = LX; Y = X; lenY = lenX; }
+  if (dtype == KSIG_DTYPE_F64)
+    return run_pde_bwd<double>(bp, X, lenX, nX, LX, Y, lenY, nY, LY, d, 1, static_kind,
+                               static_param, pairs_mode, pair_list, grad, dX, dparam,
+                               static_cast<char*>(workspace), st);
+  return run_pde_bwd<float>(bp, X, lenX, nX, LX, Y, lenY, nY, LY, d, 0, static_kind, static_param,
+                            pairs_mode, pair_list, grad, dX, dparam,
+                            static_cast<char*>(workspace), st);
 }
 
 int ksig_normalize_levels(const double* levels, int n_lev, int pairs_mode, int nX, int nY,

@@ -162,7 +162,8 @@ class SignatureBase:
                 param=float(param), levels_fn=self._levels,
                 bwd_fn=self._levels_bwd,
                 param_dtype=pt.dtype if pt is not None else torch.float64,
-                param_device=pt.device if pt is not None else 'cpu')
+                param_device=pt.device if pt is not None else 'cpu',
+                const_level0=not isinstance(self, SignaturePDEKernel))
     if sym:
       gy = None
     return AG.SigKernelFn.apply(gx, gy, pt if (pt is not None and pt.requires_grad)

@@ -101,3 +101,44 @@ def test_dp_grad_multi_strip_fp64(L):
        lambda x, y, b: OT.signature_kernel(x, y, n_levels=3, order=2,
                                            normalize=True, param=b),
        X, Y, 0.9, torch.float64, 1e-8)
+
+
+@pytest.mark.parametrize('dt,tol', [(torch.float64, 1e-8), (torch.float32, 1e-4)])
+@pytest.mark.parametrize('dyadic', [0, 1, 2])
+@pytest.mark.parametrize('normalize', [False, True])
+def test_pde_grad_rect(dt, tol, dyadic, normalize):
+  rng = np.random.default_rng(20 + dyadic)
+  X = _walks(rng, 2, 9, 3)
+  Y = _walks(rng, 2, 7, 3)
+  _run(lambda K, b: K.SignaturePDEKernel(normalize=normalize, dyadic_order=dyadic,
+                                         static_kernel=K.RBFKernel(b)),
+       lambda x, y, b: OT.signature_pde_kernel(x, y, normalize=normalize,
+                                               dyadic_order=dyadic, param=b),
+       X, Y, 0.9, dt, tol)
+
+
+def test_pde_grad_sym_fp64():
+  rng = np.random.default_rng(31)
+  X = _walks(rng, 3, 8, 2)
+  _run(lambda K, b: K.SignaturePDEKernel(normalize=True, dyadic_order=1,
+                                         static_kernel=K.RBFKernel(b)),
+       lambda x, y, b: OT.signature_pde_kernel(x, None, normalize=True,
+                                               dyadic_order=1, param=b),
+       X, None, 0.8, torch.float64, 1e-8, sym=True)
+
+
+def test_pde_grad_linear_multistrip_fp64():
+  """Column sequence longer than one strip of the adjoint (C = 2 lanes)."""
+  import os
+  os.environ['KSIG_BWD_COLS'] = '2'
+  try:
+    rng = np.random.default_rng(32)
+    X = _walks(rng, 1, 12, 2, scale=0.1)
+    Y = _walks(rng, 1, 80, 2, scale=0.05)
+    _run(lambda K, b: K.SignaturePDEKernel(normalize=False, dyadic_order=0,
+                                           static_kernel=K.LinearKernel(b)),
+         lambda x, y, b: OT.signature_pde_kernel(x, y, normalize=False,
+                                                 kind='linear', param=b),
+         X, Y, 0.7, torch.float64, 1e-8)
+  finally:
+    del os.environ['KSIG_BWD_COLS']
