@@ -257,6 +257,38 @@ def run_ours(args, rank, world, dist):
     e_step = float(t.item())
   assert Kh.shape == (N_SEQ, N_SEQ)
 
+  # Forward + backward (gradient of sum(W * K) w.r.t. X through the adjoint
+  # kernels), the 'fwd+bwd s/step' half of the metric.
+  fb_ms = None
+  if not args.no_bwd:
+    Xg = Xd.clone().requires_grad_(True)
+    Wt = torch.randn((N_SEQ, N_SEQ), device=dev, dtype=torch.float32)
+
+    def fb_step():
+      Xg.grad = None
+      Kg = kern(Xg, Yd, return_on_gpu=True)
+      (Kg * Wt).sum().backward()
+      return Xg.grad
+
+    for _ in range(2):
+      fb_step()
+    barrier()
+    fbs = []
+    for i in range(args.bwd_steps):
+      flush.fill_(i & 0xff)
+      a = torch.cuda.Event(enable_timing=True)
+      b = torch.cuda.Event(enable_timing=True)
+      a.record(stream)
+      fb_step()
+      b.record(stream)
+      b.synchronize()
+      fbs.append(a.elapsed_time(b))
+    fb_ms = sum(fbs) / len(fbs)
+    if dist is not None:
+      t = torch.tensor([fb_ms], device=dev, dtype=torch.float64)
+      dist.all_reduce(t, op=dist.ReduceOp.MAX)
+      fb_ms = float(t.item())
+
   cpu = None
   if rank == 0 and world == 1 and not args.no_cpu:
     n = args.cpu_pairs
@@ -287,6 +319,10 @@ def run_ours(args, rank, world, dist):
                 'ms_per_step': e_step,
                 'h2d_bytes_per_step': int(X.nbytes + Y.nbytes),
                 'd2h_bytes_per_step': int(N_SEQ * N_SEQ * 4)},
+        'fwd_bwd': None if fb_ms is None else {
+            's_per_step': fb_ms * 1e-3, 'ms_per_step': fb_ms,
+            'what': 'K(X, Y) forward + dL/dX backward (L = sum W*K), '
+                    'X [512, 200, 9] requires grad', 'steps': args.bwd_steps},
         'gpu_launches': int(launches),
         'clocks': clk,
         'cpu_baseline': cpu,
@@ -339,6 +375,8 @@ def main():
   ap.add_argument('--cpu-pairs', type=int, default=40)
   ap.add_argument('--ref-pairs', type=int, default=32)
   ap.add_argument('--no-cpu', action='store_true')
+  ap.add_argument('--no-bwd', action='store_true')
+  ap.add_argument('--bwd-steps', type=int, default=5)
   ap.add_argument('--n-seq', type=int, default=N_SEQ,
                   help='sequences per side; smaller values are for profiling '
                        'captures only, not bench lines')

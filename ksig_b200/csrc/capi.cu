@@ -157,11 +157,26 @@ struct FwdPlan {
   long long ntasks;
   int multi, grid, wpb;
   size_t dyn_smem;
-  long long rows_max, scratch_per_warp;
+  long long rows_max, scratch_per_warp, nwarps;
   size_t off_status, off_xr, off_yr, off_xstart, off_ystart, off_xlen, off_ylen,
       off_scratch, total;
   const KernelEntry* k;
 };
+
+// Workspace offsets of the packed points, lengths, starts and scratch.
+void layout_fwd(FwdPlan& pl, int nX, int LX, int nY, int LY) {
+  const size_t es = pl.f64 ? 8 : 4;
+  size_t off = 0;
+  pl.off_status = off; off = align_up(off + 16);
+  pl.off_xr = off; off = align_up(off + (size_t)nX * LX * pl.rs * es);
+  pl.off_yr = off; off = align_up(off + (size_t)nY * LY * pl.rs * es);
+  pl.off_xstart = off; off = align_up(off + (size_t)nX * 8);
+  pl.off_ystart = off; off = align_up(off + (size_t)nY * 8);
+  pl.off_xlen = off; off = align_up(off + (size_t)nX * 4);
+  pl.off_ylen = off; off = align_up(off + (size_t)nY * 4);
+  pl.off_scratch = off; off = align_up(off + (size_t)pl.nwarps * pl.scratch_per_warp * es);
+  pl.total = off;
+}
 
 long long num_pairs(int mode, int nX, int nY, int n_list) {
   switch (mode) {
@@ -263,17 +278,17 @@ int plan_fwd(bool pde, int nX, int LX, int nY, int LY, int d, int dtype, int n_l
   const long long nwarps = (long long)pl.grid * k->wpb;
   pl.rows_max = lx_cells > 32 ? lx_cells : 32;
   pl.scratch_per_warp = pl.multi ? pl.rows_max * pl.nx_exchange : 0;
-  size_t off = 0;
-  pl.off_status = off; off = align_up(off + 16);
-  pl.off_xr = off; off = align_up(off + (size_t)nX * LX * pl.rs * es);
-  pl.off_yr = off; off = align_up(off + (size_t)nY * LY * pl.rs * es);
-  pl.off_xstart = off; off = align_up(off + (size_t)nX * 8);
-  pl.off_ystart = off; off = align_up(off + (size_t)nY * 8);
-  pl.off_xlen = off; off = align_up(off + (size_t)nX * 4);
-  pl.off_ylen = off; off = align_up(off + (size_t)nY * 4);
-  pl.off_scratch = off; off = align_up(off + (size_t)nwarps * pl.scratch_per_warp * es);
-  pl.total = off;
+  pl.nwarps = nwarps;
+  layout_fwd(pl, nX, LX, nY, LY);
   return KSIG_OK;
+}
+
+// Re-targets a plan's packing to another kernel's padded width (the
+// adjoint kernels are compiled for their own KD set).
+void repack_for(FwdPlan& pl, int kd, int nX, int LX, int nY, int LY) {
+  pl.kd = kd;
+  pl.rs = round_up(kd + 1, pl.f64 ? 2 : 4);
+  layout_fwd(pl, nX, LX, nY, LY);
 }
 
 __global__ void starts_kernel(int64_t* start, int n, int L) {
@@ -363,6 +378,7 @@ int plan_bwd(int nX, int LX, int nY, int LY, int d, int dtype, int n_levels, int
                 "n_levels=%d order=%d", bp.f.f64 ? "f64" : "f32", d, n_levels, bp.f.p);
   bp.k = k;
   bp.c = k->c;
+  repack_for(bp.f, k->kd, nX, LX, nY, LY);
   int nh = 0;
   for (int q = 2; q <= k->nl; ++q) nh += q < bp.f.p ? q : bp.f.p;
   bp.nx = nh > 0 ? nh : 1;
@@ -461,6 +477,7 @@ int plan_pde_bwd(int nX, int LX, int nY, int LY, int d, int dtype, int dyadic, i
                 "dyadic_order=%d", bp.f.f64 ? "f64" : "f32", d, dyadic);
   bp.k = k;
   bp.c = k->c;
+  repack_for(bp.f, k->kd, nX, LX, nY, LY);
   bp.rows_max = lx > 1 ? lx : 1;
   const long long Nref = (long long)(lx > 1 ? lx : 1) * bp.F;
   const long long Mref = (long long)(ly > 1 ? ly : 1) * bp.F;
