@@ -28,6 +28,8 @@
 
 #include <cuda_pipeline.h>
 
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace ksig {
@@ -160,7 +162,19 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
 #pragma unroll
     for (int v = 0; v < RS / VN; ++v) reinterpret_cast<V*>(xv)[v] = __ldg(p + v);
   };
-  auto gram = [&](const T (&xv)[RS], T (&m)[C]) {
+  // Static-kernel values of one grid row; call sites pass a literal for RBF,
+  // so after inlining the steady loop carries no per-point select.
+  auto gram = [&](bool RBF, const T (&xv)[RS], T (&m)[C]) {
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      T acc = xv[KD] + yv[c][KD];
+#pragma unroll
+      for (int k = 0; k < KD; ++k) acc = fma(xv[k], yv[c][k], acc);
+      m[c] = RBF ? kexp2(acc) : acc;
+    }
+  };
+  // Runtime-kind version for the rare paths (one copy of the code).
+  auto gram_rt = [&](const T (&xv)[RS], T (&m)[C]) {
 #pragma unroll
     for (int c = 0; c < C; ++c) {
       T acc = xv[KD] + yv[c][KD];
@@ -192,31 +206,35 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
   }
   stage_y(nxt);
 
-  T Mcur[C], DMcur[C];
+  const bool rbf = args.kind == KIND_RBF;
+  T Mcur[C], DMcur[C], Mtmp[C], DMtmp[C];
   T xv[RS];
   load_x(cur.xb, cur.Lx, 0, xv);
-  gram(xv, Mcur);
+  gram_rt(xv, Mcur);
 #pragma unroll
   for (int c = 0; c < C; ++c) DMcur[c] = T(0);
   load_x(cur.xb, cur.Lx, 1, xv);  // Gram row of the first step
 
   // Cell work recorded at one step and executed at the next, so that a
   // step's Gram and its cell recursion form one branch-free block the
-  // compiler can interleave.  `pit` is the item of the recorded row.
+  // compiler can interleave.  The record holds the cells' Z directly.
+  // `pit` is the item of the recorded row.
   bool pv = false, plast = false;
   int pr = 0;
   Item pit = cur;
-  T pDM[C], pR = T(0);
+  T pZ[C];
 #pragma unroll
-  for (int c = 0; c < C; ++c) pDM[c] = T(0);
+  for (int c = 0; c < C; ++c) pZ[c] = T(0);
 
   int u = 0;
   int delay = lane;
   bool done = cur.task < 0;
 
-  // Cells of the recorded row + Gram of the next grid row.  `pvf` is false
-  // only when nothing was recorded (Z is forced to zero then).
-  auto main_block = [&](bool pvf, T (&Mnew)[C], T (&DMnew)[C], T& DMright) {
+  // Cells of the recorded row + Gram of the next grid row (into Mn, with
+  // vertical differences DMn against Mc).  `pvf` is false only when nothing
+  // was recorded (pZ is zero then).
+  auto main_block = [&](int rbf_c, bool pvf, const T (&Mc)[C], T (&Mn)[C], T (&DMn)[C],
+                        T& DMright) {
     T Xin[NX];
 #pragma unroll
     for (int h = 0; h < NX; ++h) Xin[h] = shfl_up(pol.X[h], 1);
@@ -229,33 +247,65 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
         pol.left_boundary(Xin);
       }
     }
-    T Z[C];
-    if (DIFF) {
-#pragma unroll
-      for (int c = 0; c < C - 1; ++c) Z[c] = pDM[c + 1] - pDM[c];
-      Z[C - 1] = pR - pDM[C - 1];
-    } else {
-      const int g0 = pit.s * STRIP + C * lane;
-#pragma unroll
-      for (int c = 0; c < C; ++c)
-        Z[c] = (pr < pit.Lx && g0 + c < pit.Ly) ? pDM[c] : T(0);
-    }
     // Lane 31's last cell belongs to the next strip when differencing.
     const bool mask_last = DIFF && lane == 31;
-    if (mask_last) Z[C - 1] = T(0);
-    pol.row(Z, Xin, mask_last, pvf, pr, ItemInfo{pit.task, pit.Lx, pit.Ly, pit.s, pit.ns}, lane);
+    pol.row(pZ, Xin, mask_last, pvf, pr, ItemInfo{pit.task, pit.Lx, pit.Ly, pit.s, pit.ns}, lane);
     if (lane == 31 && pvf && pit.s + 1 < pit.ns) {
       T* dst = bbuf + (long long)pr * NX;
 #pragma unroll
       for (int h = 0; h < NX; ++h) __stcg(dst + h, pol.X[h]);
     }
-    gram(xv, Mnew);
+    if (rbf_c < 0) gram_rt(xv, Mn);  // -1: kind decided at run time
+    else gram(rbf_c != 0, xv, Mn);
     // With differencing DM holds vertical differences of grid rows; without
     // it DM carries the previous grid row (the cells of row u-1 themselves).
 #pragma unroll
-    for (int c = 0; c < C; ++c) DMnew[c] = DIFF ? Mnew[c] - Mcur[c] : Mcur[c];
-    DMright = shfl_down(DMnew[0], 1);
+    for (int c = 0; c < C; ++c) DMn[c] = DIFF ? Mn[c] - Mc[c] : Mc[c];
+    DMright = shfl_down(DMn[0], 1);
     if (args.multi_strip) __syncwarp();
+  };
+  // Z of cell row u-1 of `cur` from its vertical differences DMc.
+  auto record = [&](const T (&DMc)[C], T DMright, bool rec) {
+    if (DIFF) {
+#pragma unroll
+      for (int c = 0; c < C - 1; ++c) pZ[c] = rec ? DMc[c + 1] - DMc[c] : T(0);
+      pZ[C - 1] = (rec && lane != 31) ? DMright - DMc[C - 1] : T(0);
+    } else {
+      const int g0 = cur.s * STRIP + C * lane;
+#pragma unroll
+      for (int c = 0; c < C; ++c)
+        pZ[c] = (rec && u - 1 < cur.Lx && g0 + c < cur.Ly) ? DMc[c] : T(0);
+    }
+  };
+  // One step of the steady loop (see below).
+  auto steady_step = [&](int rbf_c, T (&Mc)[C], T (&Mn)[C], T (&DMc)[C], T (&DMn)[C]) {
+    T DMright;
+    main_block(rbf_c, true, Mc, Mn, DMn, DMright);
+    record(DMc, DMright, true);
+    pr = u - 1;
+    ++u;
+    const bool sw = (u == cur.rows);
+    load_x(sw ? nxt.xb : cur.xb, sw ? nxt.Lx : cur.Lx, sw ? 0 : u + 1, xv);
+  };
+  auto steady_run = [&](int rbf_c, int n) {
+    int it = 0;
+    if (Policy::kUnroll2) {
+      for (; it + 1 < n; it += 2) {  // unrolled by two: Mcur/Mtmp swap roles
+        steady_step(rbf_c, Mcur, Mtmp, DMcur, DMtmp);
+        steady_step(rbf_c, Mtmp, Mcur, DMtmp, DMcur);
+      }
+    } else {
+      for (; it + 1 < n; ++it) {
+        steady_step(rbf_c, Mcur, Mtmp, DMcur, DMtmp);
+#pragma unroll
+        for (int c = 0; c < C; ++c) { Mcur[c] = Mtmp[c]; DMcur[c] = DMtmp[c]; }
+      }
+    }
+    if (it < n) {
+      steady_step(rbf_c, Mcur, Mtmp, DMcur, DMtmp);
+#pragma unroll
+      for (int c = 0; c < C; ++c) { Mcur[c] = Mtmp[c]; DMcur[c] = DMtmp[c]; }
+    }
   };
 
   for (;;) {
@@ -269,18 +319,11 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
     {
       const bool plain = delay == 0 && !done && u >= 3 && u < cur.rows;
       const int nplain = __reduce_min_sync(FULL, plain ? cur.rows - u : 0);
-      for (int it = 0; it < nplain; ++it) {
-        T Mnew[C], DMnew[C], DMright;
-        main_block(true, Mnew, DMnew, DMright);
-#pragma unroll
-        for (int c = 0; c < C; ++c) { pDM[c] = DMcur[c]; DMcur[c] = DMnew[c]; Mcur[c] = Mnew[c]; }
-        pR = DMright;
-        pr = u - 1;
-        ++u;
-        const bool sw = (u == cur.rows);
-        load_x(sw ? nxt.xb : cur.xb, sw ? nxt.Lx : cur.Lx, sw ? 0 : u + 1, xv);
+      if (nplain > 0) {
+        if (rbf) steady_run(1, nplain);
+        else steady_run(0, nplain);
+        continue;
       }
-      if (nplain > 0) continue;
     }
 
     // ---- general step ----------------------------------------------------
@@ -298,12 +341,10 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
       }
     }
 
-    // Zero the recorded differences when nothing was recorded, so Z = 0.
 #pragma unroll
-    for (int c = 0; c < C; ++c) pDM[c] = pv ? pDM[c] : T(0);
-    pR = pv ? pR : T(0);
-    T Mnew[C], DMnew[C], DMright;
-    main_block(pv, Mnew, DMnew, DMright);
+    for (int c = 0; c < C; ++c) pZ[c] = pv ? pZ[c] : T(0);
+    T DMright;
+    main_block(-1, pv, Mcur, Mtmp, DMtmp, DMright);
 
     // End of a recorded item / pair (rare, uniform).
     const bool fin_item = pv && plast;
@@ -326,15 +367,13 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
 
     // Record cell row u-1 for the next step, advance.
     const bool rec = active && u >= 1 && cur.task >= 0;
-#pragma unroll
-    for (int c = 0; c < C; ++c) pDM[c] = rec ? DMcur[c] : pDM[c];
-    pR = rec ? DMright : pR;
+    record(DMcur, DMright, rec);
     pr = rec ? u - 1 : pr;
     plast = rec && last_row;
     pv = rec;
     if (active) {
 #pragma unroll
-      for (int c = 0; c < C; ++c) { DMcur[c] = DMnew[c]; Mcur[c] = Mnew[c]; }
+      for (int c = 0; c < C; ++c) { DMcur[c] = DMtmp[c]; Mcur[c] = Mtmp[c]; }
       ++u;
     }
     // Item switch of the position (rare, uniform).
@@ -391,6 +430,9 @@ template <typename T, int C, int NL, int P, int WPB>
 struct DpPolicy {
   using L = DpLayout<NL, P>;
   static constexpr int NX = L::NH > 0 ? L::NH : 1;
+  // Two-step unrolling of the steady loop only while the register state is
+  // small enough not to spill.
+  static constexpr bool kUnroll2 = P == 1 && (NX + 3) * C <= 40 && sizeof(T) == 4;
   T X[NX];                    // horizontal running sums (outgoing)
   T Ccol[NX][C];              // column running sums
   T Clast[C];                 // column sums of the last level's totals
@@ -424,6 +466,10 @@ struct DpPolicy {
   // apart from X, which no active neighbour reads then.
   __device__ void row(const T (&Z)[C], const T (&Xin)[NX], bool, bool, int,
                       const ItemInfo&, int) {
+    if (P == 1) {
+      row_order1(Z, Xin);
+      return;
+    }
     T H[NX];
 #pragma unroll
     for (int h = 0; h < NX; ++h) H[h] = Xin[h];
@@ -478,6 +524,32 @@ struct DpPolicy {
           for (int j = 0; j < P; ++j) Rp[i][j] = Rn[i][j];
       }
       Clast[c] += tot;
+    }
+#pragma unroll
+    for (int h = 0; h < NX; ++h) X[h] = H[h];
+  }
+
+  // Order 1: R_k = z * H_k is never materialised; the column sum of level k
+  // takes it straight in (Ccol_{k+1} += z * H_k, one FFMA), so a level costs
+  // one FADD (the horizontal prefix) and one FFMA per cell.
+  __device__ void row_order1(const T (&Z)[C], const T (&Xin)[NX]) {
+    T H[NX];
+#pragma unroll
+    for (int h = 0; h < NX; ++h) H[h] = Xin[h];
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      const T z = Z[c];
+      T Hold[NX];
+#pragma unroll
+      for (int k = 2; k <= NL; ++k) {
+        Hold[k - 2] = H[k - 2];
+        H[k - 2] += Ccol[k - 2][c];
+      }
+      if (NL >= 2) Ccol[0][c] += z;
+#pragma unroll
+      for (int k = 2; k < NL; ++k) Ccol[k - 1][c] = fma(z, Hold[k - 2], Ccol[k - 1][c]);
+      if (NL >= 2) Clast[c] = fma(z, Hold[NL - 2], Clast[c]);
+      else Clast[c] += z;
     }
 #pragma unroll
     for (int h = 0; h < NX; ++h) X[h] = H[h];
@@ -550,6 +622,7 @@ dp_fwd_kernel(const SweepArgs<T> args) {
 template <typename T, int C, int F, bool DIFF>
 struct PdePolicy {
   static constexpr int NX = 2 * F;
+  static constexpr bool kUnroll2 = C * F <= 16 && sizeof(T) == 4;
   static constexpr int STRIP = DIFF ? 32 * C - 1 : 32 * C;
   T X[NX];
   T Kr[C * F];
