@@ -105,6 +105,29 @@ int ksig_signature_kern(const void* X, const int32_t* lenX, int nX, int LX,
                         double* out_levels, void* workspace,
                         size_t workspace_bytes, void* stream);
 
+/*
+ * ksig_signature_kern without a caller workspace.  No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory (an
+ * FFI host holding only raw device pointers, a framework whose allocator
+ * owns the device memory, a loop that cannot take cudaMalloc's device-wide
+ * synchronisation).  Its scratch is a 16 MiB array compiled into the
+ * library: every GPU that loads the library holds it until the process
+ * exits.  Calls whose ksig_signature_kern_workspace(...) exceeds 16 MiB are
+ * rejected with KSIG_ERR_WORKSPACE.  It calls no cudaMalloc / cudaFree.
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture.  All calls share the array and keep the last
+ * call's contents (each call clears what must start at zero), so calls
+ * that overlap on the GPU race: order them on one stream or synchronise.
+ */
+int ksig_signature_kern_static(const void* X, const int32_t* lenX, int nX,
+                               int LX, const void* Y, const int32_t* lenY,
+                               int nY, int LY, int d, int dtype,
+                               int static_kind, double static_param,
+                               int n_levels, int order, int difference,
+                               int pairs_mode, const int32_t* pair_list,
+                               int n_list, double* out_levels, void* stream);
+
 /* Workspace (bytes) required by ksig_signature_kern_pde. */
 size_t ksig_signature_kern_pde_workspace(int nX, int LX, int nY, int LY,
                                          int d, int dtype, int dyadic_order,

@@ -67,7 +67,11 @@ _SIGNATURES = {
 }
 
 # Optional entry points bound when the library exports them.
-_OPTIONAL = {}
+_OPTIONAL = {
+    'ksig_signature_kern_static': (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _I,
+                                        _I, _I, _D, _I, _I, _I, _I, _P, _I,
+                                        _P, _P]),
+}
 
 
 class KsigError(RuntimeError):

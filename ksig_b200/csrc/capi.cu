@@ -605,6 +605,46 @@ __global__ void fp32_probe_kernel(float* out, int iters, float a, float b) {
   if (s == 12345.678f) out[0] = s;  // keeps the chains live
 }
 
+// ---- fixed device scratch for ksig_signature_kern_static -----------------
+// Some callers of this library cannot allocate device memory: a host that
+// binds the C ABI over an FFI and is handed only raw device pointers, a
+// framework whose allocator has reserved the device memory up front and
+// does not let other code call cudaMalloc, or a latency-bound loop that
+// cannot afford the device-wide synchronisation of cudaMalloc / cudaFree.
+// For them the forward DP kernel also runs out of this file-scope array.
+// Every GPU that loads the library holds it until the process exits, and
+// all calls share it.
+constexpr size_t kStaticScratchBytes = (size_t)16 << 20;  // 16 MiB
+__device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+// Device address of g_static_scratch on the current device.  In host code
+// the symbol's name is only a host-side stand-in, never a device address,
+// so it is resolved with cudaGetSymbolAddress once per device, with that
+// device current, and cached.
+void* static_scratch_ptr(cudaError_t* err) {
+  static std::mutex mu;
+  static std::vector<void*> ptrs;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    *err = e;
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  if ((int)ptrs.size() <= dev) ptrs.resize(dev + 1, nullptr);
+  if (!ptrs[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess) {
+      *err = e;
+      return nullptr;
+    }
+    ptrs[dev] = p;
+  }
+  *err = cudaSuccess;
+  return ptrs[dev];
+}
+
 }  // namespace
 }  // namespace ksig
 
@@ -665,6 +705,31 @@ int ksig_signature_kern_pde(const void* X, const int32_t* lenX, int nX, int LX, 
   return fwd_entry(true, X, lenX, nX, LX, Y, lenY, nY, LY, d, dtype, static_kind, static_param,
                    0, dyadic_order, difference, pairs_mode, pair_list, n_list, out, workspace,
                    workspace_bytes, stream);
+}
+
+int ksig_signature_kern_static(const void* X, const int32_t* lenX, int nX, int LX,
+                               const void* Y, const int32_t* lenY, int nY, int LY, int d,
+                               int dtype, int static_kind, double static_param, int n_levels,
+                               int order, int difference, int pairs_mode,
+                               const int32_t* pair_list, int n_list, double* out_levels,
+                               void* stream) {
+  int rc = check_common(X, Y, pairs_mode, pair_list, n_list, static_kind, static_param);
+  if (rc) return rc;
+  FwdPlan pl;
+  rc = plan_fwd(false, nX, LX, nY, LY, d, dtype, n_levels, order, difference, pairs_mode,
+                n_list, pl);
+  if (rc) return rc;
+  if (pl.total > kStaticScratchBytes)
+    return fail(KSIG_ERR_WORKSPACE,
+                "this call needs %zu bytes of scratch, more than the %zu-byte static scratch "
+                "of ksig_signature_kern_static; call ksig_signature_kern with a workspace",
+                pl.total, kStaticScratchBytes);
+  cudaError_t e = cudaSuccess;
+  void* ws = static_scratch_ptr(&e);
+  if (!ws) return cuda_fail(e, "cudaGetSymbolAddress(g_static_scratch)");
+  return fwd_entry(false, X, lenX, nX, LX, Y, lenY, nY, LY, d, dtype, static_kind, static_param,
+                   n_levels, order, difference, pairs_mode, pair_list, n_list, out_levels, ws,
+                   kStaticScratchBytes, stream);
 }
 
 size_t ksig_signature_kern_bwd_workspace(int nX, int LX, int nY, int LY, int d, int dtype,
