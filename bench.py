@@ -234,6 +234,26 @@ def run_ours(args, rank, world, dist):
     with open(tpath) as f:
       traffic = json.load(f).get('bytes_per_launch')
 
+  # The plain FP32 one-pair-per-block baseline kernel on the same 512 x 512
+  # level computation (the 'plain' side of 'mixed vs plain FP32').
+  plain_ms = None
+  if not args.no_plain:
+    E.sig_levels_plain(Xs, Ys, Lb.PAIRS_FULL, N_LEVELS, ORDER, Lb.STATIC_RBF,
+                       BANDWIDTH)
+    torch.cuda.synchronize()
+    pm = []
+    for _ in range(2):
+      flush.fill_(2)
+      a = torch.cuda.Event(enable_timing=True)
+      b = torch.cuda.Event(enable_timing=True)
+      a.record(stream)
+      E.sig_levels_plain(Xs, Ys, Lb.PAIRS_FULL, N_LEVELS, ORDER,
+                         Lb.STATIC_RBF, BANDWIDTH)
+      b.record(stream)
+      b.synchronize()
+      pm.append(a.elapsed_time(b))
+    plain_ms = sum(pm) / len(pm)
+
   # End to end through the public API from pinned host memory.
   Xh = torch.as_tensor(X).pin_memory()
   Yh = torch.as_tensor(Y).pin_memory()
@@ -319,6 +339,11 @@ def run_ours(args, rank, world, dist):
                 'ms_per_step': e_step,
                 'h2d_bytes_per_step': int(X.nbytes + Y.nbytes),
                 'd2h_bytes_per_step': int(N_SEQ * N_SEQ * 4)},
+        'plain_fp32': None if plain_ms is None else {
+            'kernel_ms': plain_ms, 'fused_kernel_ms': k_ms,
+            'speedup': plain_ms / k_ms,
+            'what': 'plain FP32 one-pair-per-block kernel '
+                    '(ksig_signature_kern_plain) on the same 512x512 levels'},
         'fwd_bwd': None if fb_ms is None else {
             's_per_step': fb_ms * 1e-3, 'ms_per_step': fb_ms,
             'what': 'K(X, Y) forward + dL/dX backward (L = sum W*K), '
@@ -376,6 +401,7 @@ def main():
   ap.add_argument('--ref-pairs', type=int, default=32)
   ap.add_argument('--no-cpu', action='store_true')
   ap.add_argument('--no-bwd', action='store_true')
+  ap.add_argument('--no-plain', action='store_true')
   ap.add_argument('--bwd-steps', type=int, default=5)
   ap.add_argument('--n-seq', type=int, default=N_SEQ,
                   help='sequences per side; smaller values are for profiling '

@@ -128,6 +128,27 @@ int ksig_signature_kern_static(const void* X, const int32_t* lenX, int nX,
                                int pairs_mode, const int32_t* pair_list,
                                int n_list, double* out_levels, void* stream);
 
+/*
+ * Plain FP32 one-pair-per-block form of ksig_signature_kern (difference=1):
+ * the measurement baseline the fused sweep is compared with.  No reference
+ * counterpart as an entry point: it evaluates the reference's recursion
+ * (ksig/algorithms.py:47-140) as a direct CUDA translation, one CTA per
+ * pair with Z and the level states materialised in workspace scratch.
+ * Same arguments and output as ksig_signature_kern; order <= 4.
+ */
+size_t ksig_signature_kern_plain_workspace(int nX, int LX, int nY, int LY,
+                                           int d, int dtype, int n_levels,
+                                           int order, int pairs_mode,
+                                           int n_list);
+int ksig_signature_kern_plain(const void* X, const int32_t* lenX, int nX,
+                              int LX, const void* Y, const int32_t* lenY,
+                              int nY, int LY, int d, int dtype,
+                              int static_kind, double static_param,
+                              int n_levels, int order, int pairs_mode,
+                              const int32_t* pair_list, int n_list,
+                              double* out_levels, void* workspace,
+                              size_t workspace_bytes, void* stream);
+
 /* Workspace (bytes) required by ksig_signature_kern_pde. */
 size_t ksig_signature_kern_pde_workspace(int nX, int LX, int nY, int LY,
                                          int d, int dtype, int dyadic_order,

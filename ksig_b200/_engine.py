@@ -81,6 +81,28 @@ def sig_levels(X, Y, mode, n_levels, order, difference, kind, param,
   return out
 
 
+def sig_levels_plain(X, Y, mode, n_levels, order, kind, param):
+  """Per-level kernels from the plain one-pair-per-block baseline kernel."""
+  lib = L.lib()
+  Yv = X if Y is None else Y
+  dt = _dtype_code(X.data)
+  P = num_pairs(mode, X.n, Yv.n, 0)
+  out = torch.empty((n_levels + 1, max(P, 0)), dtype=torch.float64,
+                    device=X.data.device)
+  ws_bytes = lib.ksig_signature_kern_plain_workspace(
+      X.n, X.L, Yv.n, Yv.L, X.d, dt, n_levels, order, mode, 0)
+  if ws_bytes == 0:
+    L.check(L.ERR_UNSUPPORTED if 'no compiled' in L.last_error()
+            else L.ERR_INVALID)
+  ws = _workspace(ws_bytes, X.data.device)
+  rc = lib.ksig_signature_kern_plain(
+      _ptr(X.data), _ptr(X.lengths), X.n, X.L, _ptr(Yv.data),
+      _ptr(Yv.lengths), Yv.n, Yv.L, X.d, dt, kind, float(param), n_levels,
+      order, mode, None, 0, _ptr(out), _ptr(ws), ws_bytes, _stream())
+  L.check(rc)
+  return out
+
+
 def sig_levels_bwd(X, Y, mode, n_levels, order, kind, param, grad_levels,
                    dX=None, want_dparam=True, pair_list=None):
   """Row-side adjoint of :func:`sig_levels`.

@@ -36,7 +36,7 @@ NVCC_FLAGS = ['-O3', '-std=c++17', '-Xcompiler', '-fPIC',
 def _wants_lineinfo(src):
   name = os.path.basename(src)
   return name == 'capi.cu' or name.startswith(('inst_dp_f32', 'inst_pde_f32'))
-WPB = 4  # warps per block of the sweep kernels
+WPB = 2  # warps per block of the sweep kernels
 
 KD_ALL = [2, 4, 6, 8, 9, 10, 12, 16, 24, 32]
 KD_MID = [2, 4, 8, 9, 12, 16, 32]

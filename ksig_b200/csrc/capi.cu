@@ -17,6 +17,7 @@
 #include "sweep.cuh"
 #include "dp_bwd.cuh"
 #include "pde_bwd.cuh"
+#include "plain.cuh"
 
 namespace ksig {
 namespace {
@@ -548,6 +549,74 @@ int run_pde_bwd(const PdeBwdPlan& bp, const void* X, const int32_t* lenX, int nX
   return KSIG_OK;
 }
 
+// Plain one-pair-per-block baseline: the forward packing plus per-CTA
+// scratch for Z, one temporary and two sets of p^2 level-state arrays.
+struct PlainPlan {
+  FwdPlan f;
+  int grid, order;
+  long long cap;
+  size_t off_scratch, total;
+};
+
+int plan_plain(int nX, int LX, int nY, int LY, int d, int dtype, int n_levels, int order,
+               int pairs_mode, int n_list, PlainPlan& pp) {
+  int rc = plan_fwd(false, nX, LX, nY, LY, d, dtype, n_levels, order, 1, pairs_mode, n_list,
+                    pp.f);
+  if (rc) return rc;
+  if (pairs_mode == KSIG_PAIRS_UPPER || pairs_mode == KSIG_PAIRS_DIAG) { nY = nX; LY = LX; }
+  pp.order = pp.f.p;
+  if (pp.order > 4) return fail(KSIG_ERR_UNSUPPORTED, "plain baseline supports order <= 4");
+  const long long lx = LX > 1 ? LX - 1 : 1, ly = LY > 1 ? LY - 1 : 1;
+  pp.cap = lx * ly;
+  const size_t es = pp.f.f64 ? 8 : 4;
+  const long long per_cta = pp.cap * (2 + 2LL * pp.order * pp.order) * (long long)es;
+  const int sms = sm_count() > 0 ? sm_count() : 148;
+  long long grid = (long long)sms * 4;
+  const long long budget = (long long)env_int("KSIG_PLAIN_SCRATCH_MB", 8192) << 20;
+  if (grid * per_cta > budget) grid = budget / per_cta > 1 ? budget / per_cta : 1;
+  if (grid > pp.f.ntasks) grid = pp.f.ntasks > 0 ? pp.f.ntasks : 1;
+  pp.grid = (int)grid;
+  pp.off_scratch = pp.f.off_scratch;
+  pp.total = align_up(pp.off_scratch + (size_t)grid * per_cta);
+  if (pp.total < pp.f.total) pp.total = pp.f.total;
+  return KSIG_OK;
+}
+
+template <typename T>
+int run_plain(const PlainPlan& pp, const void* X, const int32_t* lenX, int nX, int LX,
+              const void* Y, const int32_t* lenY, int nY, int LY, int d, int src_f64, int kind,
+              double param, int n_levels, int mode, const int32_t* list, double* out, char* ws,
+              cudaStream_t st) {
+  const FwdPlan& pl = pp.f;
+  int* status = reinterpret_cast<int*>(ws + pl.off_status);
+  T* xr = reinterpret_cast<T*>(ws + pl.off_xr);
+  T* yr = reinterpret_cast<T*>(ws + pl.off_yr);
+  int64_t* xs = reinterpret_cast<int64_t*>(ws + pl.off_xstart);
+  int64_t* ys = reinterpret_cast<int64_t*>(ws + pl.off_ystart);
+  int32_t* xl = reinterpret_cast<int32_t*>(ws + pl.off_xlen);
+  int32_t* yl = reinterpret_cast<int32_t*>(ws + pl.off_ylen);
+  const bool self = mode == KSIG_PAIRS_UPPER || mode == KSIG_PAIRS_DIAG;
+  int rc = pack<T>(X, lenX, nX, LX, d, src_f64, kind, param, 1, pl, xr, xs, xl, status, st);
+  if (rc) return rc;
+  if (self) rc = pack<T>(X, lenX, nX, LX, d, src_f64, kind, param, 0, pl, yr, ys, yl, status, st);
+  else rc = pack<T>(Y, lenY, nY, LY, d, src_f64, kind, param, 0, pl, yr, ys, yl, status, st);
+  if (rc) return rc;
+  PlainArgs<T> a{};
+  a.xr = xr; a.xstart = xs; a.xlen = xl; a.yr = yr; a.ystart = ys; a.ylen = yl;
+  a.rs = pl.rs; a.kd = pl.kd;
+  a.mode = mode; a.nY = self ? nX : nY;
+  a.list = reinterpret_cast<const int2*>(list);
+  a.ntasks = (int)pl.ntasks; a.nX = nX; a.nYseq = self ? nX : nY;
+  a.kind = kind; a.n_levels = n_levels; a.order = pp.order;
+  a.out = out;
+  a.scratch = reinterpret_cast<T*>(ws + pp.off_scratch);
+  a.cap = pp.cap;
+  a.status = status;
+  void* kargs[] = {&a};
+  KSIG_CUDA(launch_main((const void*)&plain_dp_kernel<T>, dim3(pp.grid), dim3(256), kargs, 0, st));
+  return KSIG_OK;
+}
+
 int check_common(const void* X, const void* Y, int pairs_mode, const int32_t* list, int n_list,
                  int static_kind, double static_param) {
   if (!X) return fail(KSIG_ERR_INVALID, "X is NULL");
@@ -730,6 +799,41 @@ int ksig_signature_kern_static(const void* X, const int32_t* lenX, int nX, int L
   return fwd_entry(false, X, lenX, nX, LX, Y, lenY, nY, LY, d, dtype, static_kind, static_param,
                    n_levels, order, difference, pairs_mode, pair_list, n_list, out_levels, ws,
                    kStaticScratchBytes, stream);
+}
+
+size_t ksig_signature_kern_plain_workspace(int nX, int LX, int nY, int LY, int d, int dtype,
+                                           int n_levels, int order, int pairs_mode, int n_list) {
+  PlainPlan pp;
+  if (plan_plain(nX, LX, nY, LY, d, dtype, n_levels, order, pairs_mode, n_list, pp)) return 0;
+  return pp.total;
+}
+
+int ksig_signature_kern_plain(const void* X, const int32_t* lenX, int nX, int LX, const void* Y,
+                              const int32_t* lenY, int nY, int LY, int d, int dtype,
+                              int static_kind, double static_param, int n_levels, int order,
+                              int pairs_mode, const int32_t* pair_list, int n_list,
+                              double* out_levels, void* workspace, size_t workspace_bytes,
+                              void* stream) {
+  int rc = check_common(X, Y, pairs_mode, pair_list, n_list, static_kind, static_param);
+  if (rc) return rc;
+  if (!out_levels) return fail(KSIG_ERR_INVALID, "output is NULL");
+  PlainPlan pp;
+  rc = plan_plain(nX, LX, nY, LY, d, dtype, n_levels, order, pairs_mode, n_list, pp);
+  if (rc) return rc;
+  if (!workspace || workspace_bytes < pp.total)
+    return fail(KSIG_ERR_WORKSPACE, "workspace of %zu bytes is smaller than the %zu required",
+                workspace_bytes, pp.total);
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  KSIG_CUDA(cudaMemsetAsync(workspace, 0, 16, st));
+  if (pp.f.ntasks == 0) return KSIG_OK;
+  if (pairs_mode == KSIG_PAIRS_UPPER || pairs_mode == KSIG_PAIRS_DIAG) { nY = nX; LY = LX; Y = X; lenY = lenX; }
+  if (dtype == KSIG_DTYPE_F64)
+    return run_plain<double>(pp, X, lenX, nX, LX, Y, lenY, nY, LY, d, 1, static_kind,
+                             static_param, n_levels, pairs_mode, pair_list, out_levels,
+                             static_cast<char*>(workspace), st);
+  return run_plain<float>(pp, X, lenX, nX, LX, Y, lenY, nY, LY, d, 0, static_kind, static_param,
+                          n_levels, pairs_mode, pair_list, out_levels,
+                          static_cast<char*>(workspace), st);
 }
 
 size_t ksig_signature_kern_bwd_workspace(int nX, int LX, int nY, int LY, int d, int dtype,

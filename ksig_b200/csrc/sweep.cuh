@@ -277,6 +277,14 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
         pZ[c] = (rec && u - 1 < cur.Lx && g0 + c < cur.Ly) ? DMc[c] : T(0);
     }
   };
+  // Gram x row of the position two steps ahead (after u+1), for the
+  // two-deep x prefetch of the unrolled steady loop.
+  auto load_x2 = [&](T (&dst)[RS]) {
+    const int u1 = u + 1;
+    if (u1 < cur.rows) load_x(cur.xb, cur.Lx, u1 + 1, dst);
+    else if (u1 == cur.rows) load_x(nxt.xb, nxt.Lx, 0, dst);
+    else load_x(nxt.xb, nxt.Lx, 1, dst);
+  };
   // One step of the steady loop (see below).
   auto steady_step = [&](int rbf_c, T (&Mc)[C], T (&Mn)[C], T (&DMc)[C], T (&DMn)[C]) {
     T DMright;
@@ -287,12 +295,37 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
     const bool sw = (u == cur.rows);
     load_x(sw ? nxt.xb : cur.xb, sw ? nxt.Lx : cur.Lx, sw ? 0 : u + 1, xv);
   };
+  // Same, with this step's x row in xa, refilled afterwards with the row two
+  // steps ahead (hides the strided row loads behind a whole step).
+  auto steady_step2 = [&](int rbf_c, T (&Mc)[C], T (&Mn)[C], T (&DMc)[C], T (&DMn)[C],
+                          T (&xa)[RS]) {
+#pragma unroll
+    for (int k = 0; k < RS; ++k) xv[k] = xa[k];
+    T DMright;
+    main_block(rbf_c, true, Mc, Mn, DMn, DMright);
+    record(DMc, DMright, true);
+    pr = u - 1;
+    ++u;
+    load_x2(xa);
+  };
   auto steady_run = [&](int rbf_c, int n) {
     int it = 0;
     if (Policy::kUnroll2) {
-      for (; it + 1 < n; it += 2) {  // unrolled by two: Mcur/Mtmp swap roles
-        steady_step(rbf_c, Mcur, Mtmp, DMcur, DMtmp);
-        steady_step(rbf_c, Mtmp, Mcur, DMtmp, DMcur);
+      if (n >= 2) {
+        // xa: this step's row (in xv now); xb2: the next step's row.
+        T xa[RS], xb2[RS];
+#pragma unroll
+        for (int k = 0; k < RS; ++k) xa[k] = xv[k];
+        {
+          const bool sw = (u + 1 == cur.rows);
+          load_x(sw ? nxt.xb : cur.xb, sw ? nxt.Lx : cur.Lx, sw ? 0 : u + 2, xb2);
+        }
+        for (; it + 1 < n; it += 2) {  // unrolled by two: buffers swap roles
+          steady_step2(rbf_c, Mcur, Mtmp, DMcur, DMtmp, xa);
+          steady_step2(rbf_c, Mtmp, Mcur, DMtmp, DMcur, xb2);
+        }
+#pragma unroll
+        for (int k = 0; k < RS; ++k) xv[k] = xa[k];  // the next step's row
       }
     } else {
       for (; it + 1 < n; ++it) {

@@ -235,3 +235,21 @@ def test_api_errors():
     k(np.zeros((2, 4, 2)))
   with pytest.raises(ValueError):
     k(np.zeros((2, 4, 3, 1)))
+
+
+@pytest.mark.parametrize('order,n_levels', [(1, 5), (2, 4)])
+def test_plain_baseline_kernel_matches_oracle(order, n_levels):
+  """The plain one-pair-per-block baseline computes the same levels."""
+  from ksig_b200 import _engine as E, _lib as Lb
+  rng = np.random.default_rng(70 + order)
+  X = _walks(rng, 3, 50, 3).astype(np.float32)
+  Y = _walks(rng, 4, 37, 3).astype(np.float32)
+  ref = O.signature_kernel(X.astype(np.float64), Y.astype(np.float64),
+                           n_levels=n_levels, order=order, param=0.8,
+                           return_levels=True)
+  got = E.sig_levels_plain(E.Seqs(torch.as_tensor(X, device='cuda')),
+                           E.Seqs(torch.as_tensor(Y, device='cuda')),
+                           Lb.PAIRS_FULL, n_levels, order, Lb.STATIC_RBF, 0.8)
+  got = got.cpu().numpy().reshape(ref.shape)
+  scale = np.abs(ref).max(axis=(1, 2), keepdims=True)
+  assert np.max(np.abs(got - ref) / scale) < 1e-5
