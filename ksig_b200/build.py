@@ -81,7 +81,7 @@ def instances():
   for f, kd in itertools.product([1, 2, 4, 8], KD_FEW):
     add(('pdeb', 'f64', kd, 2, 0, f, 1))
   # DP backward (row-side gradients).
-  for dt, cs, kds in (('f32', [2, 4], KD_MID), ('f64', [2], KD_FEW)):
+  for dt, cs, kds in (('f32', [2, 4, 7], KD_MID), ('f64', [2], KD_FEW)):
     for nl, kd, c in itertools.product(NL_ALL, kds, cs):
       add(('dpb', dt, kd, c, nl, 1, 1))
     for nl, kd in itertools.product([2, 3, 4, 5, 6, 8], kds):

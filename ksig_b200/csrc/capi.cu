@@ -358,6 +358,7 @@ struct BwdPlan {
   FwdPlan f;
   const KernelEntry* k;
   int c, nx, ns_max, rows_max, grid;
+  size_t dyn_smem;
   long long scratch_per_warp;
   size_t off_scratch, total;
 };
@@ -371,9 +372,22 @@ int plan_bwd(int nX, int LX, int nY, int LY, int d, int dtype, int n_levels, int
     return fail(KSIG_ERR_UNSUPPORTED, "gradients need difference=True");
   if (pairs_mode == KSIG_PAIRS_UPPER || pairs_mode == KSIG_PAIRS_DIAG) { nY = nX; LY = LX; }
   const int ly = LY - 1, lx = LX - 1;
+  // Column count: fewest lane-steps per row, ns(C) * C, over the compiled
+  // variants (ties go to the wider strip: fewer strips, fewer records).
   const int forced = env_int("KSIG_BWD_COLS", 0);
-  int want = forced > 0 ? forced : (ly <= 63 ? 2 : 4);
-  const KernelEntry* k = find_kernel(OP_DP_BWD, bp.f.f64, d, want, n_levels, bp.f.p, 1);
+  const KernelEntry* k = nullptr;
+  long long best_cost = -1;
+  for (int want : {8, 7, 6, 5, 4, 3, 2, 1}) {
+    if (forced > 0 && want != forced) continue;
+    const KernelEntry* e = find_kernel(OP_DP_BWD, bp.f.f64, d, want, n_levels, bp.f.p, 1);
+    if (!e || e->c != want) continue;
+    const int strip = 32 * e->c - 1;
+    const long long ns = ly <= strip ? 1 : (ly + strip - 1) / strip;
+    const long long cost = ns * e->c;
+    if (best_cost < 0 || cost < best_cost) { best_cost = cost; k = e; }
+  }
+  if (!k && forced > 0)
+    k = find_kernel(OP_DP_BWD, bp.f.f64, d, forced, n_levels, bp.f.p, 1);
   if (!k)
     return fail(KSIG_ERR_UNSUPPORTED, "no compiled DP backward kernel for dtype=%s d=%d "
                 "n_levels=%d order=%d", bp.f.f64 ? "f64" : "f32", d, n_levels, bp.f.p);
@@ -386,18 +400,23 @@ int plan_bwd(int nX, int LX, int nY, int LY, int d, int dtype, int n_levels, int
   const int strip = 32 * bp.c - 1;
   bp.ns_max = ly <= strip ? 1 : (ly + strip - 1) / strip;
   bp.rows_max = lx > 1 ? lx : 1;
+  const size_t es = bp.f.f64 ? 8 : 4;
+  bp.dyn_smem = dp_bwd_smem_bytes(k->wpb, bp.c, bp.f.rs, es);
+  cudaError_t e = ensure_smem_attr(k->func, bp.dyn_smem);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(dp backward)");
   int occ = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k->func, k->wpb * 32, 0);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k->func, k->wpb * 32, bp.dyn_smem);
   if (e != cudaSuccess || occ <= 0) occ = 1;
   const int sms = sm_count() > 0 ? sm_count() : 148;
   long long warps = (long long)sms * occ * k->wpb;
   if (warps > bp.f.ntasks) warps = bp.f.ntasks > 0 ? bp.f.ntasks : 1;
+  bp.scratch_per_warp = dp_bwd_scratch_elems(bp.ns_max, bp.rows_max, bp.nx, bp.c);
+  // The per-step records grow with the strip count and the row count; keep
+  // the whole scratch within a bounded budget by running fewer warps.
+  const long long budget = (long long)env_int("KSIG_DP_BWD_SCRATCH_MB", 16384) << 20;
+  const long long cap = budget / (long long)(bp.scratch_per_warp * es);
+  if (warps > cap) warps = cap > (long long)k->wpb ? cap : k->wpb;
   bp.grid = (int)((warps + k->wpb - 1) / k->wpb);
-  const size_t es = bp.f.f64 ? 8 : 4;
-  bp.scratch_per_warp = bp.ns_max > 1
-      ? ((long long)bp.ns_max * bp.rows_max + bp.rows_max) * bp.nx +
-            (long long)bp.ns_max * 32 * bp.nx * bp.c
-      : 0;
   bp.off_scratch = bp.f.off_scratch;  // the forward scratch region is unused here
   bp.total = align_up(bp.off_scratch + (size_t)bp.grid * k->wpb * bp.scratch_per_warp * es);
   if (bp.total < bp.f.total) bp.total = bp.f.total;
@@ -429,6 +448,7 @@ int run_bwd(const BwdPlan& bp, const void* X, const int32_t* lenX, int nX, int L
   a.mode = mode;
   a.nY = self ? nX : nY;
   a.list = reinterpret_cast<const int2*>(list);
+  a.order = nullptr;
   a.ntasks = (int)pl.ntasks;
   a.nX = nX;
   a.nYseq = self ? nX : nY;
@@ -440,13 +460,13 @@ int run_bwd(const BwdPlan& bp, const void* X, const int32_t* lenX, int nX, int L
   a.LX = LX;
   a.d = d;
   a.dparam = dparam;
-  a.scratch = bp.scratch_per_warp ? reinterpret_cast<T*>(ws + bp.off_scratch) : nullptr;
+  a.scratch = reinterpret_cast<T*>(ws + bp.off_scratch);
   a.scratch_per_warp = bp.scratch_per_warp;
   a.ns_max = bp.ns_max;
   a.rows_max = bp.rows_max;
   a.status = status;
   void* kargs[] = {&a};
-  KSIG_CUDA(launch_main(bp.k->func, dim3(bp.grid), dim3(bp.k->wpb * 32), kargs, 0, st));
+  KSIG_CUDA(launch_main(bp.k->func, dim3(bp.grid), dim3(bp.k->wpb * 32), kargs, bp.dyn_smem, st));
   return KSIG_OK;
 }
 

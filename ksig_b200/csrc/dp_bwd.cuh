@@ -14,13 +14,28 @@
 // kernel (RBF: dM/dx = M (y - x) / s^2, dM/ds = M |x - y|^2 / s^3; linear:
 // dM/dx = s y, dM/ds = M / s) into dX and dparam.
 //
-// One warp per pair, all lanes on the same cell row.  Phase 1 sweeps the
-// rows top-down and keeps the final column sums (per strip).  Phase 2 sweeps
-// bottom-up: it recovers every forward prefix at row i by subtracting row i
-// from the column sums (no stored activations), forms the adjoint with
-// column suffix sums held per lane and horizontal suffix sums from warp
-// scans, and accumulates the gradient of grid row i+1.  Strips wider than
-// 32*C-1 cells exchange per-row carries through global scratch.
+// One warp per pair, skewed like the forward sweep: lane l owns C adjacent
+// columns of a strip of 32*C-1 cells.
+//
+// Phase 1 runs the forward top-down with lane l one row behind lane l-1
+// (horizontal prefixes handed on by __shfl_up).  Every lane records, per
+// step, the horizontal prefixes it received (coalesced, [step][h][lane]);
+// the final column sums stay in registers (last strip) or go to scratch.
+//
+// Phase 2 is the exact time reversal of phase 1: lane l is now one row
+// behind lane l+1.  Per cell row it
+//   - recovers the forward state at the row by subtracting the row's
+//     contributions from the column sums, with the left-boundary prefixes
+//     read back from the record (no per-cell activations are stored);
+//   - forms the adjoint: column suffix sums stay in the lane's registers,
+//     horizontal suffixes arrive from lane l+1 by __shfl_down;
+//   - pulls Zbar back to Mbar and into dX for the grid row it completes.
+//     Lane l covers its C grid columns plus the next lane's first one
+//     (partial Mbar from its own cells); the per-row dX vector is summed
+//     along the lanes by __shfl_down and added once per row and strip.
+// Order 1 takes one left-to-right pass per row (the horizontal suffix of a
+// row is the lane total minus a running prefix); order p >= 2 records the
+// cell coefficients left to right and runs the adjoint right to left.
 #pragma once
 
 #include "common.cuh"
@@ -38,6 +53,7 @@ struct DpBwdArgs {
   const int32_t* ylen;
   int mode, nY;
   const int2* list;
+  const int* order;      // optional task permutation (longest first)
   int ntasks, nX, nYseq;
   int kind;
   double param;
@@ -46,107 +62,67 @@ struct DpBwdArgs {
   T* dX;                 // [nX, LX, d] row-side gradient (accumulated)
   int LX, d;
   double* dparam;        // scalar (accumulated), may be null
-  T* scratch;
+  T* scratch;            // per warp, see dp_bwd_scratch_elems
   long long scratch_per_warp;
   int ns_max, rows_max;
   int* status;
 };
 
-// Inclusive warp scan (prefix over lanes 0..lane) of one value.
-template <typename T>
-__device__ __forceinline__ T warp_prefix_incl(T v, int lane) {
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const T y = __shfl_up_sync(FULL, v, o);
-    if (lane >= o) v += y;
-  }
-  return v;
+// Scratch elements per warp:
+//   REC [ns_max][rows_max + 33][NX][32]  phase-1 incoming prefixes per step
+//   CS  [ns_max][NX][C][32]              final column sums per strip
+//   BL  [2][rows_max][NX]                forward strip-to-strip carries
+//   BR  [2][rows_max][NX]                adjoint strip-to-strip carries
+__host__ __device__ inline long long dp_bwd_scratch_elems(int ns_max, int rows_max, int nx,
+                                                          int c) {
+  return (long long)ns_max * (rows_max + 33) * nx * 32 + (long long)ns_max * nx * c * 32 +
+         4LL * rows_max * nx;
 }
 
-// Inclusive warp suffix scan (over lanes lane..31) of one value.
-template <typename T>
-__device__ __forceinline__ T warp_suffix_incl(T v, int lane) {
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const T y = __shfl_down_sync(FULL, v, o);
-    if (lane + o < 32) v += y;
-  }
-  return v;
+// Dynamic shared memory per block: each lane keeps its C + 1 packed column
+// points of the current strip in shared memory ([C+1][RV][32] 16-byte
+// vectors per warp) instead of registers.
+__host__ __device__ inline size_t dp_bwd_smem_bytes(int wpb, int c, int rs, size_t es) {
+  return (size_t)wpb * (c + 1) * (rs * es / 16) * 32 * 16;
 }
-
-// Reduces VP values (VP a power of two <= 32) over the warp; afterwards lane
-// l holds the total of value index red_index<VP>(l).
-template <int VP>
-__device__ __forceinline__ int red_index(int lane) {
-  int idx = 0, n = VP;
-#pragma unroll
-  for (int o = 16; o >= 1; o >>= 1) {
-    if (n > 1) {
-      n >>= 1;
-      if (lane & o) idx += n;
-    }
-  }
-  return idx;
-}
-
-template <typename T, int VP>
-__device__ __forceinline__ T transpose_reduce(T (&v)[VP], int lane) {
-  int n = VP;
-#pragma unroll
-  for (int o = 16; o >= 1; o >>= 1) {
-    if (n > 1) {
-      const int half = n >> 1;
-      const bool up = (lane & o) != 0;
-#pragma unroll
-      for (int i = 0; i < VP / 2; ++i) {
-        if (i < half) {
-          const T send = up ? v[i] : v[i + half];
-          const T keep = up ? v[i + half] : v[i];
-          v[i] = keep + __shfl_xor_sync(FULL, send, o);
-        }
-      }
-      n = half;
-    } else {
-      v[0] += __shfl_xor_sync(FULL, v[0], o);
-    }
-  }
-  return v[0];
-}
-
-template <int N>
-struct Pow2Up { static constexpr int v = N <= 1 ? 1 : 2 * Pow2Up<(N + 1) / 2>::v; };
-template <> struct Pow2Up<1> { static constexpr int v = 1; };
 
 template <typename T, int KD, int C, int NL, int P, int WPB>
 __global__ void __launch_bounds__(WPB * 32)
 dp_bwd_kernel(const DpBwdArgs<T> args) {
   using Lay = DpLayout<NL, P>;
-  constexpr int NX = Lay::NH > 0 ? Lay::NH : 1;
+  constexpr int NH = Lay::NH;
+  constexpr int NX = NH > 0 ? NH : 1;
   constexpr int RS = packed_stride<T>(KD);
   constexpr int VN = Vec<T>::N;
+  constexpr int RV = RS / VN;
   using V = typename Vec<T>::type;
   constexpr int STRIP = 32 * C - 1;
-  constexpr int VP = Pow2Up<KD>::v;
-  // Per-cell forward coefficients kept between the two passes of a row:
-  // for level k the coefficient of Z in each state R_k[r][s].
-  constexpr int NCOEF = 1 + (NL >= 2 ? (NL - 1) * P * P : 0);
+  constexpr int NCOEF = P == 1 ? 1 : 1 + (NL >= 2 ? (NL - 1) * P * P : 0);
 
+  extern __shared__ __align__(16) unsigned char dsm[];
   const int lane = threadIdx.x & 31;
-  const long long wg = (long long)blockIdx.x * WPB + (threadIdx.x >> 5);
+  const int wib = threadIdx.x >> 5;
+  V* ysm = reinterpret_cast<V*>(dsm) + (size_t)wib * (C + 1) * RV * 32;
+  const long long wg = (long long)blockIdx.x * WPB + wib;
   const long long nw = (long long)gridDim.x * WPB;
-  T* scr = args.scratch ? args.scratch + wg * args.scratch_per_warp : nullptr;
-  // Scratch layout (multi-strip only): BL[ns_max][rows_max][NX] forward
-  // carries, BR[rows_max][NX] adjoint carries, CS[ns_max][32][NX][C] final
-  // column sums per strip.
-  T* BL = scr;
-  T* BR = scr ? scr + (long long)args.ns_max * args.rows_max * NX : nullptr;
-  T* CS = scr ? BR + (long long)args.rows_max * NX : nullptr;
+  T* scr = args.scratch + wg * args.scratch_per_warp;
+  const long long steps_max = (long long)args.rows_max + 33;
+  const long long rm = args.rows_max;
+  T* REC = scr;
+  T* CS = REC + (long long)args.ns_max * steps_max * NX * 32;
+  T* BL = CS + (long long)args.ns_max * NX * C * 32;
+  T* BR = BL + 2 * rm * NX;
 
   const double alpha = 1.4426950408889634 / fmax(2.0 * args.param * args.param, 1e-12);
   const bool rbf = args.kind == KIND_RBF;
+  const bool want_dpar = args.dparam != nullptr;
+  const T inv2a = T(1.0 / (2.0 * alpha));
+  const double xscale = rbf ? 1.0 / (args.param * args.param) : args.param;
+  double dpar_w = 0.0;
 
   for (long long tid = wg; tid < args.ntasks; tid += nw) {
-    int2 ab = decode_task((int)tid, args.mode, args.nY, args.list, nullptr);
+    const int2 ab = decode_task((int)tid, args.mode, args.nY, args.list, args.order);
+    const int task = args.order ? args.order[tid] : (int)tid;
     if (ab.x < 0 || ab.x >= args.nX || ab.y < 0 || ab.y >= args.nYseq) {
       if (lane == 0) set_status(args.status, KSIG_ERR_INVALID);
       continue;
@@ -156,337 +132,395 @@ dp_bwd_kernel(const DpBwdArgs<T> args) {
     const int lx = Lx - 1, ly = Ly - 1;
     if (lx <= 0 || ly <= 0) continue;  // no cells: levels >= 1 are constant
     const int ns = (ly + STRIP - 1) / STRIP;
-    if (ns > 1 && (!scr || ns > args.ns_max || lx > args.rows_max)) {
+    if (ns > args.ns_max || lx > args.rows_max) {
       if (lane == 0) set_status(args.status, KSIG_ERR_DEVICE);
       continue;
     }
     T w[NL + 1];
 #pragma unroll
     for (int k = 0; k <= NL; ++k)
-      w[k] = (k >= 1 && k <= args.nl_out) ? (T)args.glev[(long long)k * args.ntasks + tid] : T(0);
+      w[k] = (k >= 1 && k <= args.nl_out) ? (T)args.glev[(long long)k * args.ntasks + task] : T(0);
 
     const T* xb = args.xr + args.xstart[a] * RS;
     const T* yb = args.yr + args.ystart[b] * RS;
-    T yv[C][KD + 1];
-    auto load_y = [&](int s) {
+    // Column points of strip s (C own columns + the next lane's first).
+    auto stage_y = [&](int s) {
 #pragma unroll
-      for (int c = 0; c < C; ++c) {
+      for (int c = 0; c <= C; ++c) {
         int col = s * STRIP + C * lane + c;
         col = col < Ly - 1 ? col : Ly - 1;
         const V* p = reinterpret_cast<const V*>(yb + (long long)col * RS);
-        T tmp[RS];
 #pragma unroll
-        for (int v = 0; v < RS / VN; ++v) reinterpret_cast<V*>(tmp)[v] = __ldg(p + v);
-#pragma unroll
-        for (int k = 0; k <= KD; ++k) yv[c][k] = tmp[k];
+        for (int v = 0; v < RV; ++v) ysm[(c * RV + v) * 32 + lane] = __ldg(p + v);
       }
     };
+    auto y_col = [&](int c, T (&yv)[RS]) {
+#pragma unroll
+      for (int v = 0; v < RV; ++v) reinterpret_cast<V*>(yv)[v] = ysm[(c * RV + v) * 32 + lane];
+    };
     auto load_x = [&](int row, T (&xv)[RS]) {
-      row = row < Lx - 1 ? row : Lx - 1;
+      row = row < 0 ? 0 : (row > lx ? lx : row);
       const V* p = reinterpret_cast<const V*>(xb + (long long)row * RS);
 #pragma unroll
-      for (int v = 0; v < RS / VN; ++v) reinterpret_cast<V*>(xv)[v] = __ldg(p + v);
+      for (int v = 0; v < RV; ++v) reinterpret_cast<V*>(xv)[v] = __ldg(p + v);
     };
-    auto gram = [&](const T (&xv)[RS], T (&m)[C], T (&arg)[C]) {
+    auto gram_row = [&](const T (&xv)[RS], T (&m)[C], T (&arg)[C]) {
 #pragma unroll
       for (int c = 0; c < C; ++c) {
-        T acc = xv[KD] + yv[c][KD];
+        T yv[RS];
+        y_col(c, yv);
+        T acc = xv[KD] + yv[KD];
 #pragma unroll
-        for (int k = 0; k < KD; ++k) acc = fma(xv[k], yv[c][k], acc);
+        for (int k = 0; k < KD; ++k) acc = fma(xv[k], yv[k], acc);
         arg[c] = acc;
         m[c] = static_value(acc, args.kind);
       }
     };
-    // Z of cell row r from grid rows r (Mlo) and r+1 (Mhi); masks the cell
-    // that belongs to the next strip.
-    auto cells = [&](const T (&Mlo)[C], const T (&Mhi)[C], T (&Z)[C]) {
-      T DM[C];
-#pragma unroll
-      for (int c = 0; c < C; ++c) DM[c] = Mhi[c] - Mlo[c];
-      const T right = shfl_down(DM[0], 1);
-#pragma unroll
-      for (int c = 0; c < C - 1; ++c) Z[c] = DM[c + 1] - DM[c];
-      Z[C - 1] = lane == 31 ? T(0) : right - DM[C - 1];
-    };
+    auto rec_at = [&](int s, long long t) { return REC + ((long long)s * steps_max + t) * NX * 32; };
 
-    T CC[NX][C];  // forward column sums (rows < i) of A / V inputs
+    T Ccol[NX][C];  // forward column sums (rows above the current row)
 
     // ---------------- phase 1: forward, top-down, strips left to right -----
     for (int s = 0; s < ns; ++s) {
-      load_y(s);
+      stage_y(s);
 #pragma unroll
       for (int h = 0; h < NX; ++h)
 #pragma unroll
-        for (int c = 0; c < C; ++c) CC[h][c] = T(0);
-      T xv[RS], Mlo[C], Mhi[C], argd[C];
-      load_x(0, xv);
-      gram(xv, Mlo, argd);
-      for (int r = 0; r < lx; ++r) {
-        load_x(r + 1, xv);
-        gram(xv, Mhi, argd);
+        for (int c = 0; c < C; ++c) Ccol[h][c] = T(0);
+      T Xout[NX];
+#pragma unroll
+      for (int h = 0; h < NX; ++h) Xout[h] = T(0);
+      T Mprev[C], DMold[C];
+#pragma unroll
+      for (int c = 0; c < C; ++c) { Mprev[c] = T(0); DMold[c] = T(0); }
+      T xc[RS];
+      load_x(-lane, xc);
+      const T* blin = BL + (long long)((s + 1) & 1) * rm * NX;  // written by strip s - 1
+      T* blout = BL + (long long)(s & 1) * rm * NX;
+      const int T1 = lx + 33;
+      for (int t = 0; t < T1; ++t) {
+        const int rho = t - lane;     // grid row computed this step
+        const int r = rho - 2;        // cell row processed this step
+        const bool act = r >= 0 && r < lx;
+        T xn[RS];
+        load_x(rho + 1, xn);
+        T Mnew[C], argn[C];
+        gram_row(xc, Mnew, argn);
+        T DMnew[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) DMnew[c] = Mnew[c] - Mprev[c];
+        // Lane l+1 has just formed the vertical difference of cell row r.
+        const T right = shfl_down(DMnew[0], 1);
+        T Xin[NX];
+#pragma unroll
+        for (int h = 0; h < NX; ++h) Xin[h] = shfl_up(Xout[h], 1);
+        if (lane == 0) {
+#pragma unroll
+          for (int h = 0; h < NX; ++h) Xin[h] = (s > 0 && act) ? blin[(long long)r * NX + h] : T(0);
+        }
         T Z[C];
-        cells(Mlo, Mhi, Z);
-        // Carry-in of horizontal sums from the strip to the left.
-        T carry[NX];
+#pragma unroll
+        for (int c = 0; c < C - 1; ++c) Z[c] = DMold[c + 1] - DMold[c];
+        Z[C - 1] = lane == 31 ? T(0) : right - DMold[C - 1];
+#pragma unroll
+        for (int c = 0; c < C; ++c)
+          if (!act || s * STRIP + C * lane + c >= ly) Z[c] = T(0);
+        if (act && NH > 0) {
+          T* rp = rec_at(s, t);
+#pragma unroll
+          for (int h = 0; h < NX; ++h) rp[h * 32 + lane] = Xin[h];
+        }
+        // Forward cell recursion (same arithmetic as DpPolicy::row).
+        T H[NX];
+#pragma unroll
+        for (int h = 0; h < NX; ++h) H[h] = Xin[h];
+        if (P == 1) {
+#pragma unroll
+          for (int c = 0; c < C; ++c) {
+            const T z = Z[c];
+            T Hold[NX];
+#pragma unroll
+            for (int k = 2; k <= NL; ++k) {
+              Hold[k - 2] = H[k - 2];
+              H[k - 2] += Ccol[k - 2][c];
+            }
+            if (NL >= 2) Ccol[0][c] += z;
+#pragma unroll
+            for (int k = 2; k < NL; ++k) Ccol[k - 1][c] = fma(z, Hold[k - 2], Ccol[k - 1][c]);
+          }
+        } else {
+#pragma unroll
+          for (int c = 0; c < C; ++c) {
+            const T z = Z[c];
+            T Rp[P][P];
+#pragma unroll
+            for (int i = 0; i < P; ++i)
+#pragma unroll
+              for (int j = 0; j < P; ++j) Rp[i][j] = T(0);
+            Rp[0][0] = z;
+            T tot = z;
+#pragma unroll
+            for (int k = 2; k <= NL; ++k) {
+              const int f = Lay::f(k), fp = Lay::f(k - 1), o = Lay::off(k);
+              T Rn[P][P];
+#pragma unroll
+              for (int i = 0; i < P; ++i)
+#pragma unroll
+                for (int j = 0; j < P; ++j) Rn[i][j] = T(0);
+              Rn[0][0] = z * H[o];
+              H[o] += Ccol[o][c];
+              Ccol[o][c] += tot;
+              T lsum = Rn[0][0];
+#pragma unroll
+              for (int rr = 1; rr < P; ++rr) {
+                if (rr < f) {
+                  T Vs = T(0), Us = T(0);
+#pragma unroll
+                  for (int i = 0; i < P; ++i)
+                    if (i < fp) { Vs += Rp[i][rr - 1]; Us += Rp[rr - 1][i]; }
+                  const T zr = z * (T(1) / T(rr + 1));
+                  Rn[0][rr] = zr * Ccol[o + rr][c];
+                  Ccol[o + rr][c] += Vs;
+                  Rn[rr][0] = zr * H[o + rr];
+                  H[o + rr] += Us;
+                  lsum += Rn[0][rr] + Rn[rr][0];
+#pragma unroll
+                  for (int ss = 1; ss < P; ++ss) {
+                    if (ss < f) {
+                      Rn[rr][ss] = z * (T(1) / T((rr + 1) * (ss + 1))) * Rp[rr - 1][ss - 1];
+                      lsum += Rn[rr][ss];
+                    }
+                  }
+                }
+              }
+              tot = lsum;
+#pragma unroll
+              for (int i = 0; i < P; ++i)
+#pragma unroll
+                for (int j = 0; j < P; ++j) Rp[i][j] = Rn[i][j];
+            }
+          }
+        }
+#pragma unroll
+        for (int h = 0; h < NX; ++h) Xout[h] = H[h];
+        if (lane == 31 && act && s + 1 < ns) {
+#pragma unroll
+          for (int h = 0; h < NX; ++h) blout[(long long)r * NX + h] = Xout[h];
+        }
+#pragma unroll
+        for (int c = 0; c < C; ++c) { Mprev[c] = Mnew[c]; DMold[c] = DMnew[c]; }
+#pragma unroll
+        for (int k = 0; k < RS; ++k) xc[k] = xn[k];
+      }
+      if (ns > 1 && s + 1 < ns) {
+        T* dst = CS + (long long)s * NX * C * 32;
 #pragma unroll
         for (int h = 0; h < NX; ++h)
-          carry[h] = (s > 0) ? BL[((long long)s * args.rows_max + r) * NX + h] : T(0);
-        // 2-D prefixes: exclusive prefix over columns of CC (rows < r).
-        T Hs[NX];  // per-lane exclusive carry for each horizontal quantity
-        T tot[NX];
 #pragma unroll
-        for (int h = 0; h < NX; ++h) {
-          T t = T(0);
+          for (int c = 0; c < C; ++c) dst[(h * C + c) * 32 + lane] = Ccol[h][c];
+      }
+      __syncwarp();  // carries and records of this strip -> later readers
+    }
+
+    // ---------------- phase 2: adjoint, bottom-up, strips right to left ----
+    for (int s = ns - 1; s >= 0; --s) {
+      stage_y(s);
+      if (s != ns - 1) {
+        const T* src = CS + (long long)s * NX * C * 32;
 #pragma unroll
-          for (int c = 0; c < C; ++c) t += CC[h][c];
-          tot[h] = t;
+        for (int h = 0; h < NX; ++h)
+#pragma unroll
+          for (int c = 0; c < C; ++c) Ccol[h][c] = src[(h * C + c) * 32 + lane];
+      }
+      T E[NX][C];  // adjoint column suffix sums (rows below the current row)
+#pragma unroll
+      for (int h = 0; h < NX; ++h)
+#pragma unroll
+        for (int c = 0; c < C; ++c) E[h][c] = T(0);
+      T Mprev[C], argprev[C], Zbprev[C];
+#pragma unroll
+      for (int c = 0; c < C; ++c) { Mprev[c] = T(0); argprev[c] = T(0); Zbprev[c] = T(0); }
+      T DMlast0 = T(0), mr_old = T(0), ar_old = T(0);
+      T accprev[KD + 1];
+#pragma unroll
+      for (int k = 0; k <= KD; ++k) accprev[k] = T(0);
+      T Aprev[NX];
+#pragma unroll
+      for (int h = 0; h < NX; ++h) Aprev[h] = T(0);
+      const T* brin = BR + (long long)((s + 1) & 1) * rm * NX;  // written by strip s + 1
+      T* brout = BR + (long long)(s & 1) * rm * NX;
+      T xc[RS];
+      load_x(lx + 31 - lane, xc);
+      // Record of the row this lane processes next (prefetched one step).
+      T recn[NX];
+      {
+        const int rho0 = -(31 - lane);
+        const bool act0 = rho0 >= 1 && rho0 <= lx;
+#pragma unroll
+        for (int h = 0; h < NX; ++h)
+          recn[h] = (act0 && NH > 0) ? rec_at(s, lx + 33)[h * 32 + lane] : T(0);
+      }
+      const int T2 = lx + 33;
+      for (int u = 0; u < T2; ++u) {
+        const int rho = u - (31 - lane);
+        const int g = lx - rho;                      // grid row computed; cell row processed
+        const bool act = rho >= 1 && rho <= lx;      // cell row g exists
+        const bool fin = rho >= 1 && rho <= lx + 1;  // grid row g + 1 completes here
+        // Values lane l+1 produced one step earlier (same rows).
+        const T right = shfl_down(DMlast0, 1);
+        const T mr_new = shfl_down(Mprev[0], 1);
+        const T ar_new = shfl_down(argprev[0], 1);
+        T Ain[NX];
+#pragma unroll
+        for (int h = 0; h < NX; ++h) Ain[h] = shfl_down(Aprev[h], 1);
+        T acc[KD + 1];
+#pragma unroll
+        for (int k = 0; k <= KD; ++k) acc[k] = shfl_down(accprev[k], 1);
+        if (lane == 31) {
+#pragma unroll
+          for (int k = 0; k <= KD; ++k) acc[k] = T(0);
+#pragma unroll
+          for (int h = 0; h < NX; ++h)
+            Ain[h] = (s + 1 < ns && act) ? brin[(long long)g * NX + h] : T(0);
         }
-        // S2 parts (index off(k)) are known at row start; row-prefix parts
-        // (off(k)+r') need this row's values and are scanned per level.
+        T Xin[NX];
 #pragma unroll
-        for (int k = 2; k <= NL; ++k) {
-          const int o = Lay::off(k);
-          const T inc = warp_prefix_incl(tot[o], lane);
-          Hs[o] = inc - tot[o] + carry[o];
-          if (lane == 31 && s + 1 < ns) BL[((long long)(s + 1) * args.rows_max + r) * NX + o] = inc + carry[o];
+        for (int h = 0; h < NX; ++h) Xin[h] = recn[h];
+        {
+          const bool actn = rho + 1 >= 1 && rho + 1 <= lx;
+          const long long tn = (long long)lx + 33 - (u + 1);
+#pragma unroll
+          for (int h = 0; h < NX; ++h)
+            recn[h] = (actn && NH > 0) ? rec_at(s, tn)[h * 32 + lane] : T(0);
         }
-        // Per-cell recursion with per-level row-prefix scans.
-        T Rst[C][P][P];
-        T Utot[P];
+        T xn[RS];
+        load_x(g - 1, xn);
+        T Mnew[C], argn[C];
+        gram_row(xc, Mnew, argn);
+        T DMnew[C];
 #pragma unroll
-        for (int c = 0; c < C; ++c) {
+        for (int c = 0; c < C; ++c) DMnew[c] = Mprev[c] - Mnew[c];
+        T Z[C];
 #pragma unroll
-          for (int i = 0; i < P; ++i)
+        for (int c = 0; c < C - 1; ++c) Z[c] = DMnew[c + 1] - DMnew[c];
+        Z[C - 1] = lane == 31 ? T(0) : right - DMnew[C - 1];
 #pragma unroll
-            for (int j = 0; j < P; ++j) Rst[c][i][j] = T(0);
-          Rst[c][0][0] = Z[c];
-        }
+        for (int c = 0; c < C; ++c)
+          if (!act || s * STRIP + C * lane + c >= ly) Z[c] = T(0);
+
+        T Zb[C];
+        T Aout[NX];
+        T H[NX];
 #pragma unroll
-        for (int k = 2; k <= NL; ++k) {
-          const int f = Lay::f(k), fp = Lay::f(k - 1), o = Lay::off(k);
-          // Row prefixes of U_r (current row values of the previous level).
-          T Uv[C][P];
+        for (int h = 0; h < NX; ++h) H[h] = Xin[h];
+        if (P == 1) {
+          // Q[h]: running Rbar of level h+1 (suffix over the columns right of
+          // the current one); Aout: everything from this lane's first column.
+          T Q[NX];
 #pragma unroll
-          for (int rr = 1; rr < P; ++rr) {
-            if (rr < f) {
-              T t = T(0);
+          for (int h = 0; h < NX; ++h) {
+            T tsum = T(0);
 #pragma unroll
-              for (int c = 0; c < C; ++c) {
-                T u = T(0);
-#pragma unroll
-                for (int i = 0; i < P; ++i)
-                  if (i < fp) u += Rst[c][rr - 1][i];
-                Uv[c][rr] = u;
-                t += u;
-              }
-              Utot[rr] = t;
-              const T inc = warp_prefix_incl(t, lane);
-              Hs[o + rr] = inc - t + carry[o + rr];
-              if (lane == 31 && s + 1 < ns)
-                BL[((long long)(s + 1) * args.rows_max + r) * NX + o + rr] = inc + carry[o + rr];
-            }
+            for (int c = 0; c < C; ++c) tsum += E[h][c];
+            Aout[h] = Ain[h] + tsum;
+            Q[h] = w[h + 1] + Aout[h];
           }
 #pragma unroll
           for (int c = 0; c < C; ++c) {
             const T z = Z[c];
-            T A = T(0);
+            // Forward state at (g, c): undo the row's column-sum updates.
+            T cf[NX];
+            T cprev = T(1);
 #pragma unroll
-            for (int i = 0; i < P; ++i)
-#pragma unroll
-              for (int j = 0; j < P; ++j)
-                if (i < fp && j < fp) A += Rst[c][i][j];
-            T Rn[P][P];
-#pragma unroll
-            for (int i = 0; i < P; ++i)
-#pragma unroll
-              for (int j = 0; j < P; ++j) Rn[i][j] = T(0);
-            Rn[0][0] = z * Hs[o];
-            Hs[o] += CC[o][c];
-            CC[o][c] += A;
-#pragma unroll
-            for (int rr = 1; rr < P; ++rr) {
-              if (rr < f) {
-                T Vs = T(0);
-#pragma unroll
-                for (int i = 0; i < P; ++i)
-                  if (i < fp) Vs += Rst[c][i][rr - 1];
-                const T zr = z * (T(1) / T(rr + 1));
-                Rn[0][rr] = zr * CC[o + rr][c];
-                CC[o + rr][c] += Vs;
-                Rn[rr][0] = zr * Hs[o + rr];
-                Hs[o + rr] += Uv[c][rr];
-#pragma unroll
-                for (int ss = 1; ss < P; ++ss)
-                  if (ss < f)
-                    Rn[rr][ss] = z * (T(1) / T((rr + 1) * (ss + 1))) * Rst[c][rr - 1][ss - 1];
-              }
+            for (int k = 2; k <= NL; ++k) {
+              Ccol[k - 2][c] = fma(-z, cprev, Ccol[k - 2][c]);
+              cf[k - 2] = H[k - 2];
+              H[k - 2] += Ccol[k - 2][c];
+              cprev = cf[k - 2];
             }
+            // Adjoint, top level down.
+            T rb_next = w[NL];
+            T zb;
+            if constexpr (NL >= 2) zb = rb_next * cf[NL - 2];
+            else zb = rb_next;
 #pragma unroll
-            for (int i = 0; i < P; ++i)
-#pragma unroll
-              for (int j = 0; j < P; ++j) Rst[c][i][j] = Rn[i][j];
+            for (int k = NL - 1; k >= 1; --k) {
+              Q[k - 1] -= E[k - 1][c];
+              const T rb = Q[k - 1];
+              E[k - 1][c] = fma(z, rb_next, E[k - 1][c]);
+              zb = (k >= 2) ? fma(rb, cf[k >= 2 ? k - 2 : 0], zb) : zb + rb;
+              rb_next = rb;
+            }
+            Zb[c] = zb;
           }
-        }
-#pragma unroll
-        for (int c = 0; c < C; ++c) Mlo[c] = Mhi[c];
-      }
-      if (ns > 1) {
-        T* dst = CS + (((long long)s * 32 + lane) * NX) * C;
-#pragma unroll
-        for (int h = 0; h < NX; ++h)
-#pragma unroll
-          for (int c = 0; c < C; ++c) dst[h * C + c] = CC[h][c];
-        __syncwarp();  // carries of lane 31 -> all lanes of the next strip
-      }
-    }
-
-    // ---------------- phase 2: adjoint, bottom-up, strips right to left ----
-    double dpar = 0.0;
-    for (int s = ns - 1; s >= 0; --s) {
-      load_y(s);
-      if (ns > 1) {
-        const T* src = CS + (((long long)s * 32 + lane) * NX) * C;
-#pragma unroll
-        for (int h = 0; h < NX; ++h)
-#pragma unroll
-          for (int c = 0; c < C; ++c) CC[h][c] = src[h * C + c];
-      }
-      T DA[NX][C];   // adjoint column suffix sums (rows > i)
-#pragma unroll
-      for (int h = 0; h < NX; ++h)
-#pragma unroll
-        for (int c = 0; c < C; ++c) DA[h][c] = T(0);
-      const int g0 = s * STRIP + C * lane;
-      T xv[RS], Mhi[C], arghi[C], Zbhi[C];
-      load_x(lx, xv);
-      gram(xv, Mhi, arghi);
-#pragma unroll
-      for (int c = 0; c < C; ++c) Zbhi[c] = T(0);
-      T xhi[RS];
-#pragma unroll
-      for (int k = 0; k < RS; ++k) xhi[k] = xv[k];
-      for (int r = lx - 1; r >= -1; --r) {
-        T Mlo[C], arglo[C], Zb[C];
-        T xlo[RS];
-        if (r >= 0) {
-          load_x(r, xlo);
-          gram(xlo, Mlo, arglo);
-          T Z[C];
-          cells(Mlo, Mhi, Z);
-          T carry[NX], bcarry[NX];
-#pragma unroll
-          for (int h = 0; h < NX; ++h) {
-            carry[h] = (s > 0) ? BL[((long long)s * args.rows_max + r) * NX + h] : T(0);
-            bcarry[h] = (s + 1 < ns) ? BR[(long long)r * NX + h] : T(0);
-          }
-          // ---- ascending: recover the forward prefixes at row r ----
+        } else {
+          // Left to right: forward state and the coefficient of z in every
+          // state of every level.
           T coef[C][NCOEF];
-          T Rst[C][P][P];
 #pragma unroll
           for (int c = 0; c < C; ++c) {
+            const T z = Z[c];
+            T Rp[P][P];
 #pragma unroll
             for (int i = 0; i < P; ++i)
 #pragma unroll
-              for (int j = 0; j < P; ++j) Rst[c][i][j] = T(0);
-            Rst[c][0][0] = Z[c];
+              for (int j = 0; j < P; ++j) Rp[i][j] = T(0);
+            Rp[0][0] = z;
+            T tot = z;
             coef[c][0] = T(1);
-          }
 #pragma unroll
-          for (int k = 2; k <= NL; ++k) {
-            const int f = Lay::f(k), fp = Lay::f(k - 1), o = Lay::off(k);
-            const int cb = 1 + (k - 2) * P * P;
-            // Column sums back to rows < r.
-#pragma unroll
-            for (int c = 0; c < C; ++c) {
-              T A = T(0);
+            for (int k = 2; k <= NL; ++k) {
+              const int f = Lay::f(k), fp = Lay::f(k - 1), o = Lay::off(k);
+              const int cb = 1 + (k - 2) * P * P;
+              T Rn[P][P], cf[P][P];
 #pragma unroll
               for (int i = 0; i < P; ++i)
 #pragma unroll
-                for (int j = 0; j < P; ++j)
-                  if (i < fp && j < fp) A += Rst[c][i][j];
-              CC[o][c] -= A;
+                for (int j = 0; j < P; ++j) { Rn[i][j] = T(0); cf[i][j] = T(0); }
+              Ccol[o][c] -= tot;
+              cf[0][0] = H[o];
+              Rn[0][0] = z * H[o];
+              H[o] += Ccol[o][c];
+              T lsum = Rn[0][0];
 #pragma unroll
               for (int rr = 1; rr < P; ++rr) {
                 if (rr < f) {
-                  T Vs = T(0);
+                  T Vs = T(0), Us = T(0);
 #pragma unroll
                   for (int i = 0; i < P; ++i)
-                    if (i < fp) Vs += Rst[c][i][rr - 1];
-                  CC[o + rr][c] -= Vs;
+                    if (i < fp) { Vs += Rp[i][rr - 1]; Us += Rp[rr - 1][i]; }
+                  const T inv = T(1) / T(rr + 1);
+                  const T zr = z * inv;
+                  Ccol[o + rr][c] -= Vs;
+                  cf[0][rr] = Ccol[o + rr][c] * inv;
+                  Rn[0][rr] = zr * Ccol[o + rr][c];
+                  cf[rr][0] = H[o + rr] * inv;
+                  Rn[rr][0] = zr * H[o + rr];
+                  H[o + rr] += Us;
+                  lsum += Rn[0][rr] + Rn[rr][0];
+#pragma unroll
+                  for (int ss = 1; ss < P; ++ss) {
+                    if (ss < f) {
+                      const T inv2 = T(1) / T((rr + 1) * (ss + 1));
+                      cf[rr][ss] = Rp[rr - 1][ss - 1] * inv2;
+                      Rn[rr][ss] = z * inv2 * Rp[rr - 1][ss - 1];
+                      lsum += Rn[rr][ss];
+                    }
+                  }
                 }
               }
-            }
-            T t = T(0);
-#pragma unroll
-            for (int c = 0; c < C; ++c) t += CC[o][c];
-            T H2 = warp_prefix_incl(t, lane) - t + carry[o];
-            T HU[P], Uv[C][P];
-#pragma unroll
-            for (int rr = 1; rr < P; ++rr) {
-              HU[rr] = T(0);
-              if (rr < f) {
-                T tu = T(0);
-#pragma unroll
-                for (int c = 0; c < C; ++c) {
-                  T u = T(0);
-#pragma unroll
-                  for (int i = 0; i < P; ++i)
-                    if (i < fp) u += Rst[c][rr - 1][i];
-                  Uv[c][rr] = u;
-                  tu += u;
-                }
-                HU[rr] = warp_prefix_incl(tu, lane) - tu + carry[o + rr];
-              }
-            }
-#pragma unroll
-            for (int c = 0; c < C; ++c) {
-              const T z = Z[c];
-              T cf[P][P];
-#pragma unroll
-              for (int i = 0; i < P; ++i)
-#pragma unroll
-                for (int j = 0; j < P; ++j) cf[i][j] = T(0);
-              cf[0][0] = H2;
-              H2 += CC[o][c];
-#pragma unroll
-              for (int rr = 1; rr < P; ++rr) {
-                if (rr < f) {
-                  cf[0][rr] = CC[o + rr][c] * (T(1) / T(rr + 1));
-                  cf[rr][0] = HU[rr] * (T(1) / T(rr + 1));
-                  HU[rr] += Uv[c][rr];
-#pragma unroll
-                  for (int ss = 1; ss < P; ++ss)
-                    if (ss < f) cf[rr][ss] = Rst[c][rr - 1][ss - 1] * (T(1) / T((rr + 1) * (ss + 1)));
-                }
-              }
+              tot = lsum;
 #pragma unroll
               for (int i = 0; i < P; ++i)
 #pragma unroll
                 for (int j = 0; j < P; ++j) {
+                  Rp[i][j] = Rn[i][j];
                   coef[c][cb + i * P + j] = cf[i][j];
-                  Rst[c][i][j] = z * cf[i][j];
                 }
             }
           }
-          // ---- descending: adjoint at row r ----
-          // Horizontal suffixes of the column suffix sums DA (rows > r) for
-          // the 2-D prefix adjoints, all levels at once.
-          T Abar[NX];
-#pragma unroll
-          for (int k = 2; k <= NL; ++k) {
-            const int o = Lay::off(k);
-            T t = T(0);
-#pragma unroll
-            for (int c = 0; c < C; ++c) t += DA[o][c];
-            const T inc = warp_suffix_incl(t, lane);
-            Abar[o] = inc - t + bcarry[o];
-            if (lane == 0 && s > 0) BR[(long long)r * NX + o] = inc + bcarry[o];
-          }
+          // Right to left: the adjoint, top level down.
           T Rb_next[C][P][P];
-          T Ub[P];
-          // Column-suffix increments of the level processed last: they are
-          // added to DA only after the next lower level has read DA, so that
-          // every suffix used in row r covers rows > r only.
           T pendDA[P][C];
 #pragma unroll
           for (int c = 0; c < C; ++c) Zb[c] = T(0);
@@ -496,26 +530,13 @@ dp_bwd_kernel(const DpBwdArgs<T> args) {
             const int fn = (k < NL) ? Lay::f(k + 1) : 0;
             const int on = (k < NL) ? Lay::off(k + 1) : 0;
             const int cb = 1 + (k - 2) * P * P;
-            // Suffix (exclusive, over j' > j) of the next level's row-adjoint
-            // inputs, per r'.
-            T Ab = (k < NL) ? Abar[on] : T(0);
+            T Ab = (k < NL) ? Ain[on] : T(0);
+            T Ub[P];
 #pragma unroll
-            for (int rr = 1; rr < P; ++rr) Ub[rr] = T(0);
-            if (k < NL) {
-#pragma unroll
-              for (int rr = 1; rr < P; ++rr) {
-                if (rr < fn) {
-                  T tu = T(0);
-#pragma unroll
-                  for (int c = 0; c < C; ++c)
-                    tu += Z[c] * (T(1) / T(rr + 1)) * Rb_next[c][rr][0];
-                  const T inc = warp_suffix_incl(tu, lane);
-                  Ub[rr] = inc - tu + bcarry[on + rr];
-                  if (lane == 0 && s > 0) BR[(long long)r * NX + on + rr] = inc + bcarry[on + rr];
-                }
-              }
+            for (int rr = 0; rr < P; ++rr) {
+              Ub[rr] = T(0);
+              if (k < NL && rr >= 1 && rr < fn) Ub[rr] = Ain[on + rr];
             }
-            // Right to left over the lane's cells.
 #pragma unroll
             for (int c = C - 1; c >= 0; --c) {
               const T z = Z[c];
@@ -529,7 +550,7 @@ dp_bwd_kernel(const DpBwdArgs<T> args) {
                     v = w[k];
                     if (k < NL) {
                       v += Ab;
-                      if (j + 1 < fn) v += DA[on + j + 1][c];
+                      if (j + 1 < fn) v += E[on + j + 1][c];
                       if (i + 1 < fn) v += Ub[i + 1];
                       if (i + 1 < fn && j + 1 < fn)
                         v += z * (T(1) / T((i + 2) * (j + 2))) * Rb_next[c][i + 1][j + 1];
@@ -537,7 +558,6 @@ dp_bwd_kernel(const DpBwdArgs<T> args) {
                   }
                   Rb[i][j] = v;
                 }
-              // Zbar contribution: coefficient of z in each state.
               if (k == 1) {
                 Zb[c] += Rb[0][0];
               } else {
@@ -547,9 +567,8 @@ dp_bwd_kernel(const DpBwdArgs<T> args) {
                   for (int j = 0; j < P; ++j)
                     if (i < f && j < f) Zb[c] += Rb[i][j] * coef[c][cb + i * P + j];
               }
-              // Advance the horizontal suffixes (exclusive -> include cell c).
               if (k < NL) {
-                Ab += DA[on][c];
+                Ab += E[on][c];
 #pragma unroll
                 for (int rr = 1; rr < P; ++rr)
                   if (rr < fn) Ub[rr] += z * (T(1) / T(rr + 1)) * Rb_next[c][rr][0];
@@ -559,13 +578,18 @@ dp_bwd_kernel(const DpBwdArgs<T> args) {
 #pragma unroll
                 for (int j = 0; j < P; ++j) Rb_next[c][i][j] = Rb[i][j];
             }
-            // Level k+1's increments can go in now that level k has used DA.
             if (k < NL) {
+              Aout[on] = Ab;
+#pragma unroll
+              for (int rr = 1; rr < P; ++rr)
+                if (rr < fn) Aout[on + rr] = Ub[rr];
+              // Level k+1's column increments go in now that level k has
+              // read the suffixes of the rows below.
 #pragma unroll
               for (int c = 0; c < C; ++c)
 #pragma unroll
                 for (int rr = 0; rr < P; ++rr)
-                  if (rr < fn) DA[on + rr][c] += pendDA[rr][c];
+                  if (rr < fn) E[on + rr][c] += pendDA[rr][c];
             }
             if (k >= 2) {
 #pragma unroll
@@ -577,71 +601,78 @@ dp_bwd_kernel(const DpBwdArgs<T> args) {
               }
             }
           }
-          // Cells outside the pair (padding, the next strip's cell) carry no
-          // adjoint.
+          if (NH == 0) Aout[0] = T(0);
+        }
+        // Cells outside the pair (padding, the next strip's cell) carry no
+        // adjoint.
 #pragma unroll
-          for (int c = 0; c < C; ++c) {
-            const int j = g0 + c;
-            if (r >= lx || j >= ly || (lane == 31 && c == C - 1)) Zb[c] = T(0);
+        for (int c = 0; c < C; ++c)
+          if (!act || s * STRIP + C * lane + c >= ly || (lane == 31 && c == C - 1)) Zb[c] = T(0);
+        if (lane == 0 && act && s > 0) {
+#pragma unroll
+          for (int h = 0; h < NX; ++h) brout[(long long)g * NX + h] = Aout[h];
+        }
+
+        // ---- grid row p = g + 1: partial Mbar of this lane's cells ----
+        const int p = g + 1;
+        T dp = T(0);
+#pragma unroll
+        for (int c = 0; c <= C; ++c) {
+          T mb, Mq, aq;
+          if (c < C) {
+            mb = Zbprev[c] - Zb[c];
+            if (c > 0) mb += Zb[c - 1] - Zbprev[c - 1];
+            Mq = Mprev[c];
+            aq = argprev[c];
+          } else {
+            mb = Zb[C - 1] - Zbprev[C - 1];
+            Mq = mr_old;
+            aq = ar_old;
           }
-        } else {
+          const int q = s * STRIP + C * lane + c;
+          const bool valid = fin && q < Ly && (c < C || lane < 31);
+          const T W = valid ? (rbf ? mb * Mq : mb) : T(0);
+          T yv[RS];
+          y_col(c, yv);
 #pragma unroll
-          for (int c = 0; c < C; ++c) { Zb[c] = T(0); Mlo[c] = T(0); arglo[c] = T(0); }
+          for (int k = 0; k < KD; ++k) acc[k] = fma(W, yv[k], acc[k]);
+          acc[KD] += W;
+          dp = fma(W, rbf ? aq : Mq, dp);
         }
-        // ---- Mbar on grid row r+1 and its pull-back ----
-        const T zl_lo = shfl_up(Zb[C - 1], 1);
-        const T zl_hi = shfl_up(Zbhi[C - 1], 1);
-        T q[VP];
+        if (want_dpar) dpar_w += (double)dp;
+        if (lane == 0 && fin) {
+          T xp[RS];
+          load_x(p, xp);
+          T* dst = args.dX + ((long long)a * args.LX + p) * args.d;
 #pragma unroll
-        for (int k = 0; k < VP; ++k) q[k] = T(0);
-        T sw = T(0);
-        const int gi = r + 1;  // grid row being finalised
-#pragma unroll
-        for (int c = 0; c < C; ++c) {
-          const T lo_l = (c == 0) ? (lane == 0 ? T(0) : zl_lo) : Zb[c - 1];
-          const T hi_l = (c == 0) ? (lane == 0 ? T(0) : zl_hi) : Zbhi[c - 1];
-          const T mbar = lo_l - Zb[c] - hi_l + Zbhi[c];
-          const int j = g0 + c;
-          const bool valid = j < Ly && gi < Lx;
-          const T W = valid ? (rbf ? mbar * Mhi[c] : mbar) : T(0);
-          sw += W;
-#pragma unroll
-          for (int k = 0; k < KD; ++k) q[k] = fma(W, yv[c][k], q[k]);
-          if (valid) {
-            // d/dparam: RBF M |x-y|^2 / s^3 with |x-y|^2 = -arg / alpha;
-            // linear M / s.
-            dpar += rbf ? (double)W * (-(double)arghi[c] / alpha) : (double)W * (double)Mhi[c];
-          }
-        }
-        // dX row gi: RBF (1/s^2) sum_j W (y_j - x), linear s sum_j Mbar y_j.
-        if (rbf) {
-          const T inv2a = T(1) / T(2.0 * alpha);
-#pragma unroll
-          for (int k = 0; k < KD; ++k) q[k] -= sw * (xhi[k] * inv2a);
-        }
-        const T tot = transpose_reduce<T, VP>(q, lane);
-        const int idx = red_index<VP>(lane);
-        if ((lane & (32 / VP - 1)) == 0) {  // one lane per reduced value
-          if (idx < args.d && gi < Lx) {
-            const double scale = rbf ? 1.0 / (args.param * args.param) : args.param;
-            T* dst = args.dX + ((long long)a * args.LX + gi) * args.d + idx;
-            atomicAdd(dst, (T)(scale * (double)tot));
+          for (int k = 0; k < KD; ++k) {
+            if (k < args.d) {
+              const T v = rbf ? acc[k] - acc[KD] * (xp[k] * inv2a) : acc[k];
+              atomicAdd(dst + k, (T)(xscale * (double)v));
+            }
           }
         }
 #pragma unroll
-        for (int c = 0; c < C; ++c) { Mhi[c] = Mlo[c]; arghi[c] = arglo[c]; Zbhi[c] = Zb[c]; }
+        for (int k = 0; k <= KD; ++k) accprev[k] = acc[k];
 #pragma unroll
-        for (int k = 0; k < RS; ++k) xhi[k] = xlo[k];
+        for (int h = 0; h < NX; ++h) Aprev[h] = Aout[h];
+        DMlast0 = DMnew[0];
+        mr_old = mr_new;
+        ar_old = ar_new;
+#pragma unroll
+        for (int c = 0; c < C; ++c) { Mprev[c] = Mnew[c]; argprev[c] = argn[c]; Zbprev[c] = Zb[c]; }
+#pragma unroll
+        for (int k = 0; k < RS; ++k) xc[k] = xn[k];
       }
-      if (ns > 1) __syncwarp();
+      __syncwarp();  // adjoint carries of this strip -> the next strip
     }
-    if (args.dparam) {
+  }
+  if (want_dpar) {
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) dpar += __shfl_xor_sync(FULL, dpar, o);
-      if (lane == 0) {
-        const double p = args.param;
-        atomicAdd(args.dparam, rbf ? dpar / (p * p * p) : dpar / p);
-      }
+    for (int o = 16; o > 0; o >>= 1) dpar_w += __shfl_xor_sync(FULL, dpar_w, o);
+    if (lane == 0 && dpar_w != 0.0) {
+      const double p = args.param;
+      atomicAdd(args.dparam, rbf ? -dpar_w / (alpha * p * p * p) : dpar_w / p);
     }
   }
 }
