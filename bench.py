@@ -356,6 +356,115 @@ def run_ours(args, rank, world, dist):
 
 
 # ---------------------------------------------------------------------------
+# Ragged higher-order workload (not the default bench line): N = M = 2048
+# sequences, lengths log-uniform in [32, 1024], d = 16 cumsummed N(0, 1)
+# increments, RBF bandwidth sqrt(16), n_levels = 8, order = 2, normalize.
+# Times the forward Gram and forward + input gradient through the public API
+# (ragged lists), and the fused and plain kernels on a bounded sample of the
+# same pairs.
+# ---------------------------------------------------------------------------
+
+RAGGED = dict(n=2048, lmin=32, lmax=1024, d=16, n_levels=8, order=2, bw=4.0)
+
+
+def make_ragged(n, lmin, lmax, d, seed):
+  rng = np.random.default_rng(seed)
+  lens = np.exp(rng.uniform(np.log(lmin), np.log(lmax), n)).astype(np.int64)
+  lens = np.clip(lens, lmin, lmax)
+  return [np.cumsum(rng.standard_normal((int(L), d)), 0).astype(np.float32)
+          for L in lens]
+
+
+def run_ragged(args):
+  import torch
+
+  import ksig_b200 as K
+  from ksig_b200 import _engine as E
+  from ksig_b200 import _lib as Lb
+  R = dict(RAGGED)
+  if args.n_seq is not None:
+    R['n'] = args.n_seq
+  n, m, p, bw = R['n'], R['n_levels'], R['order'], R['bw']
+  dev = torch.device('cuda', 0)
+  Xl = [torch.as_tensor(a, device=dev) for a in make_ragged(n, R['lmin'], R['lmax'], R['d'], 5)]
+  Yl = [torch.as_tensor(a, device=dev) for a in make_ragged(n, R['lmin'], R['lmax'], R['d'], 6)]
+  lx = np.array([a.shape[0] for a in Xl])
+  ly = np.array([a.shape[0] for a in Yl])
+  cells = float(np.sum(lx - 1)) * float(np.sum(ly - 1))
+  kern = K.SignatureKernel(n_levels=m, order=p, normalize=True,
+                           static_kernel=K.RBFKernel(bw))
+  W = torch.randn((n, n), device=dev, dtype=torch.float32)
+
+  def timed(fn, steps, warm):
+    for _ in range(warm):
+      fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(steps):
+      a = torch.cuda.Event(enable_timing=True)
+      b = torch.cuda.Event(enable_timing=True)
+      a.record()
+      fn()
+      b.record()
+      b.synchronize()
+      ts.append(a.elapsed_time(b))
+    return sum(ts) / len(ts)
+
+  fwd_ms = timed(lambda: kern(Xl, Yl, return_on_gpu=True), args.steps, 1)
+  Xg = [a.clone().requires_grad_(True) for a in Xl]
+
+  def fb():
+    Kg = kern(Xg, Yl, return_on_gpu=True)
+    (Kg * W).sum().backward()
+
+  fb_ms = timed(fb, args.bwd_steps, 1)
+
+  # Fused vs plain kernels on the same bounded sample of pairs.
+  s = min(args.plain_sample, n)
+  def seqs(lst):
+    L = max(a.shape[0] for a in lst)
+    data = torch.zeros((len(lst), L, R['d']), device=dev)
+    for i, a in enumerate(lst):
+      data[i, :a.shape[0]] = a
+    return E.Seqs(data, torch.tensor([a.shape[0] for a in lst], device=dev))
+  Xs, Ys = seqs(Xl[:s]), seqs(Yl[:s])
+  scells = float(np.sum(lx[:s] - 1)) * float(np.sum(ly[:s] - 1))
+  gl = torch.randn((m + 1, s * s), device=dev, dtype=torch.float64)
+  os.environ.setdefault('KSIG_PLAIN_SCRATCH_MB', '65536')
+  f_fwd = timed(lambda: E.sig_levels(Xs, Ys, Lb.PAIRS_FULL, m, p, True, Lb.STATIC_RBF, bw), 2, 1)
+  f_bwd = timed(lambda: E.sig_levels_bwd(Xs, Ys, Lb.PAIRS_FULL, m, p, Lb.STATIC_RBF, bw, gl,
+                                         want_dparam=False), 2, 1)
+  p_fwd = timed(lambda: E.sig_levels_plain(Xs, Ys, Lb.PAIRS_FULL, m, p, Lb.STATIC_RBF, bw), 1, 1)
+  p_bwd = timed(lambda: E.sig_levels_bwd_plain(Xs, Ys, Lb.PAIRS_FULL, m, p, Lb.STATIC_RBF, bw,
+                                               gl, want_dparam=False), 1, 1)
+  # FP32 levels against the FP64 path (pinned to the oracle) on a corner.
+  c = min(16, s)
+  Xc, Yc = seqs(Xl[:c]), seqs(Yl[:c])
+  l32 = E.sig_levels(Xc, Yc, Lb.PAIRS_FULL, m, p, True, Lb.STATIC_RBF, bw)
+  l64 = E.sig_levels(E.Seqs(Xc.data.double(), Xc.lengths), E.Seqs(Yc.data.double(), Yc.lengths),
+                     Lb.PAIRS_FULL, m, p, True, Lb.STATIC_RBF, bw)
+  scale = l64.abs().amax(dim=1, keepdim=True).clamp_min(1e-300)
+  rel = float(((l32 - l64).abs() / scale).max())
+  line = {
+      'metric': METRIC, 'workload': f'sig_dp_rbf_ragged_N{n}_M{n}_L32-1024_d16_m{m}_p{p}_normalized',
+      'forward': {'value': n * n / (fwd_ms * 1e-3), 'unit': UNIT, 'ms_per_step': fwd_ms,
+                  'cells_per_s': cells / (fwd_ms * 1e-3)},
+      'fwd_bwd': {'s_per_step': fb_ms * 1e-3,
+                  'what': 'K(X, Y) + d sum(W*K)/dX through the public API (ragged lists)'},
+      'sample': {'pairs': s * s, 'cells': scells,
+                 'fused_fwd_ms': f_fwd, 'fused_bwd_ms': f_bwd,
+                 'plain_fwd_ms': p_fwd, 'plain_bwd_ms': p_bwd,
+                 'speedup_fwd': p_fwd / f_fwd, 'speedup_bwd': p_bwd / f_bwd,
+                 'speedup_fwd_bwd': (p_fwd + p_bwd) / (f_fwd + f_bwd),
+                 'plain_fwd_bwd_full_s_est': (p_fwd + p_bwd) * 1e-3 * cells / scells},
+      'rel_err_fp32_vs_fp64_levels': rel,
+      'cells': cells, 'steps': args.steps, 'bwd_steps': args.bwd_steps,
+      'dtype': 'f32', 'data': 'synthetic',
+  }
+  print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
 # Reference arm: the reference recursion on the host cores.
 # ---------------------------------------------------------------------------
 
@@ -403,11 +512,16 @@ def main():
   ap.add_argument('--no-bwd', action='store_true')
   ap.add_argument('--no-plain', action='store_true')
   ap.add_argument('--bwd-steps', type=int, default=5)
-  ap.add_argument('--n-seq', type=int, default=N_SEQ,
+  ap.add_argument('--workload', default='dp512', choices=['dp512', 'ragged-dp'],
+                  help='dp512: the bench line; ragged-dp: the 2048 x 2048 ragged '
+                       'order-2 workload, printed as its own report line')
+  ap.add_argument('--plain-sample', type=int, default=96)
+  ap.add_argument('--n-seq', type=int, default=None,
                   help='sequences per side; smaller values are for profiling '
                        'captures only, not bench lines')
   args = ap.parse_args()
-  globals()['N_SEQ'] = args.n_seq
+  if args.n_seq is not None and args.workload == 'dp512':
+    globals()['N_SEQ'] = args.n_seq
   args.warmup = max(args.warmup, 3)
   world = int(os.environ.get('WORLD_SIZE', '1'))
   rank = int(os.environ.get('RANK', '0'))
@@ -425,6 +539,9 @@ def main():
     dist = tdist
   else:
     torch.cuda.set_device(0)
+  if args.workload == 'ragged-dp':
+    run_ragged(args)
+    return
   try:
     run_ours(args, rank, world, dist)
   finally:

@@ -149,6 +149,29 @@ int ksig_signature_kern_plain(const void* X, const int32_t* lenX, int nX,
                               double* out_levels, void* workspace,
                               size_t workspace_bytes, void* stream);
 
+/*
+ * Plain FP32 one-pair-per-block form of ksig_signature_kern_bwd
+ * (difference=1): the baseline of the fused adjoint.  No reference
+ * counterpart (the reference has no gradients).  One CTA per pair keeps Z,
+ * every level's states and the adjoint states as full arrays in workspace
+ * scratch and runs the adjoint recursion as array passes.  Same arguments
+ * and accumulation semantics as ksig_signature_kern_bwd without
+ * `difference`; order <= 4.
+ */
+size_t ksig_signature_kern_plain_bwd_workspace(int nX, int LX, int nY, int LY,
+                                               int d, int dtype, int n_levels,
+                                               int order, int pairs_mode,
+                                               int n_list);
+int ksig_signature_kern_plain_bwd(const void* X, const int32_t* lenX, int nX,
+                                  int LX, const void* Y, const int32_t* lenY,
+                                  int nY, int LY, int d, int dtype,
+                                  int static_kind, double static_param,
+                                  int n_levels, int order, int pairs_mode,
+                                  const int32_t* pair_list, int n_list,
+                                  const double* grad_levels, void* dX,
+                                  double* dparam, void* workspace,
+                                  size_t workspace_bytes, void* stream);
+
 /* Workspace (bytes) required by ksig_signature_kern_pde. */
 size_t ksig_signature_kern_pde_workspace(int nX, int LX, int nY, int LY,
                                          int d, int dtype, int dyadic_order,

@@ -135,6 +135,33 @@ def sig_levels_bwd(X, Y, mode, n_levels, order, kind, param, grad_levels,
   return dX, dpar
 
 
+def sig_levels_bwd_plain(X, Y, mode, n_levels, order, kind, param, grad_levels,
+                         dX=None, want_dparam=True):
+  """Row-side adjoint from the plain one-pair-per-block baseline kernel
+  (same contract as :func:`sig_levels_bwd`)."""
+  lib = L.lib()
+  Yv = X if Y is None else Y
+  dt = _dtype_code(X.data)
+  if dX is None:
+    dX = torch.zeros_like(X.data)
+  dpar = torch.zeros((1,), dtype=torch.float64, device=X.data.device) \
+      if want_dparam else None
+  gl = grad_levels.to(torch.float64).contiguous()
+  ws_bytes = lib.ksig_signature_kern_plain_bwd_workspace(
+      X.n, X.L, Yv.n, Yv.L, X.d, dt, n_levels, order, mode, 0)
+  if ws_bytes == 0:
+    L.check(L.ERR_UNSUPPORTED if 'no compiled' in L.last_error()
+            else L.ERR_INVALID)
+  ws = _workspace(ws_bytes, X.data.device)
+  rc = lib.ksig_signature_kern_plain_bwd(
+      _ptr(X.data), _ptr(X.lengths), X.n, X.L, _ptr(Yv.data),
+      _ptr(Yv.lengths), Yv.n, Yv.L, X.d, dt, kind, float(param), n_levels,
+      order, mode, None, 0, _ptr(gl), _ptr(dX), _ptr(dpar), _ptr(ws),
+      ws_bytes, _stream())
+  L.check(rc)
+  return dX, dpar
+
+
 def pde_values(X, Y, mode, dyadic_order, difference, kind, param,
                pair_list=None):
   """Signature-PDE kernel per pair ``[P]`` (float64)."""

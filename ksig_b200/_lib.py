@@ -63,6 +63,10 @@ _SIGNATURES = {
     'ksig_signature_kern_plain': (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _I, _I,
                                        _I, _D, _I, _I, _I, _P, _I, _P, _P, _SZ,
                                        _P]),
+    'ksig_signature_kern_plain_bwd_workspace': (_SZ, [_I] * 10),
+    'ksig_signature_kern_plain_bwd': (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _I,
+                                           _I, _I, _D, _I, _I, _I, _P, _I, _P,
+                                           _P, _P, _P, _SZ, _P]),
     'ksig_launch_count': (ctypes.c_ulonglong, []),
     'ksig_profile_enable': (None, [_I]),
     'ksig_profile_read': (_I, [ctypes.POINTER(ctypes.c_double),

@@ -413,7 +413,7 @@ int plan_bwd(int nX, int LX, int nY, int LY, int d, int dtype, int n_levels, int
   bp.scratch_per_warp = dp_bwd_scratch_elems(bp.ns_max, bp.rows_max, bp.nx, bp.c);
   // The per-step records grow with the strip count and the row count; keep
   // the whole scratch within a bounded budget by running fewer warps.
-  const long long budget = (long long)env_int("KSIG_DP_BWD_SCRATCH_MB", 16384) << 20;
+  const long long budget = (long long)env_int("KSIG_DP_BWD_SCRATCH_MB", 32768) << 20;
   const long long cap = budget / (long long)(bp.scratch_per_warp * es);
   if (warps > cap) warps = cap > (long long)k->wpb ? cap : k->wpb;
   bp.grid = (int)((warps + k->wpb - 1) / k->wpb);
@@ -637,6 +637,85 @@ int run_plain(const PlainPlan& pp, const void* X, const int32_t* lenX, int nX, i
   return KSIG_OK;
 }
 
+// Plain one-pair-per-block adjoint baseline: per-CTA scratch for Z, all
+// level states, two sets of p^2 adjoint states, Zbar, one temporary and the
+// grid weights, each of LX * LY elements.
+struct PlainBwdPlan {
+  PlainPlan pp;
+  int nbuf;
+};
+
+int plan_plain_bwd(int nX, int LX, int nY, int LY, int d, int dtype, int n_levels, int order,
+                   int pairs_mode, int n_list, PlainBwdPlan& bp) {
+  int rc = plan_plain(nX, LX, nY, LY, d, dtype, n_levels, order, pairs_mode, n_list, bp.pp);
+  if (rc) return rc;
+  PlainPlan& pp = bp.pp;
+  if (pairs_mode == KSIG_PAIRS_UPPER || pairs_mode == KSIG_PAIRS_DIAG) { nY = nX; LY = LX; }
+  const int p = pp.order;
+  int states = 0;
+  for (int k = 1; k <= n_levels; ++k) { const int f = k < p ? k : p; states += f * f; }
+  bp.nbuf = 1 + states + 2 * p * p + 3;
+  pp.cap = (long long)(LX > 1 ? LX : 1) * (LY > 1 ? LY : 1);
+  const size_t es = pp.f.f64 ? 8 : 4;
+  const long long per_cta = pp.cap * bp.nbuf * (long long)es;
+  const int sms = sm_count() > 0 ? sm_count() : 148;
+  long long grid = (long long)sms * 4;
+  const long long budget = (long long)env_int("KSIG_PLAIN_SCRATCH_MB", 8192) << 20;
+  if (grid * per_cta > budget) grid = budget / per_cta > 1 ? budget / per_cta : 1;
+  if (grid > pp.f.ntasks) grid = pp.f.ntasks > 0 ? pp.f.ntasks : 1;
+  pp.grid = (int)grid;
+  pp.total = align_up(pp.off_scratch + (size_t)grid * per_cta);
+  if (pp.total < pp.f.total) pp.total = pp.f.total;
+  return KSIG_OK;
+}
+
+template <typename T>
+int run_plain_bwd(const PlainBwdPlan& bp, const void* X, const int32_t* lenX, int nX, int LX,
+                  const void* Y, const int32_t* lenY, int nY, int LY, int d, int src_f64,
+                  int kind, double param, int n_levels, int mode, const int32_t* list,
+                  const double* glev, int nl_out, void* dX, double* dparam, char* ws,
+                  cudaStream_t st) {
+  const PlainPlan& pp = bp.pp;
+  const FwdPlan& pl = pp.f;
+  int* status = reinterpret_cast<int*>(ws + pl.off_status);
+  T* xr = reinterpret_cast<T*>(ws + pl.off_xr);
+  T* yr = reinterpret_cast<T*>(ws + pl.off_yr);
+  int64_t* xs = reinterpret_cast<int64_t*>(ws + pl.off_xstart);
+  int64_t* ys = reinterpret_cast<int64_t*>(ws + pl.off_ystart);
+  int32_t* xl = reinterpret_cast<int32_t*>(ws + pl.off_xlen);
+  int32_t* yl = reinterpret_cast<int32_t*>(ws + pl.off_ylen);
+  const bool self = mode == KSIG_PAIRS_UPPER || mode == KSIG_PAIRS_DIAG;
+  int rc = pack<T>(X, lenX, nX, LX, d, src_f64, kind, param, 1, pl, xr, xs, xl, status, st);
+  if (rc) return rc;
+  if (self) rc = pack<T>(X, lenX, nX, LX, d, src_f64, kind, param, 0, pl, yr, ys, yl, status, st);
+  else rc = pack<T>(Y, lenY, nY, LY, d, src_f64, kind, param, 0, pl, yr, ys, yl, status, st);
+  if (rc) return rc;
+  PlainBwdArgs<T> a{};
+  PlainArgs<T>& f = a.f;
+  f.xr = xr; f.xstart = xs; f.xlen = xl; f.yr = yr; f.ystart = ys; f.ylen = yl;
+  f.rs = pl.rs; f.kd = pl.kd;
+  f.mode = mode; f.nY = self ? nX : nY;
+  f.list = reinterpret_cast<const int2*>(list);
+  f.ntasks = (int)pl.ntasks; f.nX = nX; f.nYseq = self ? nX : nY;
+  f.kind = kind; f.n_levels = n_levels; f.order = pp.order;
+  f.out = nullptr;
+  f.scratch = reinterpret_cast<T*>(ws + pp.off_scratch);
+  f.cap = pp.cap;
+  f.status = status;
+  a.glev = glev;
+  a.nl_out = nl_out;
+  a.dX = reinterpret_cast<T*>(dX);
+  a.LX = LX;
+  a.d = d;
+  a.param = param;
+  a.dparam = dparam;
+  a.nbuf = bp.nbuf;
+  void* kargs[] = {&a};
+  KSIG_CUDA(launch_main((const void*)&plain_dp_bwd_kernel<T>, dim3(pp.grid), dim3(256), kargs,
+                        0, st));
+  return KSIG_OK;
+}
+
 int check_common(const void* X, const void* Y, int pairs_mode, const int32_t* list, int n_list,
                  int static_kind, double static_param) {
   if (!X) return fail(KSIG_ERR_INVALID, "X is NULL");
@@ -854,6 +933,45 @@ int ksig_signature_kern_plain(const void* X, const int32_t* lenX, int nX, int LX
   return run_plain<float>(pp, X, lenX, nX, LX, Y, lenY, nY, LY, d, 0, static_kind, static_param,
                           n_levels, pairs_mode, pair_list, out_levels,
                           static_cast<char*>(workspace), st);
+}
+
+size_t ksig_signature_kern_plain_bwd_workspace(int nX, int LX, int nY, int LY, int d,
+                                               int dtype, int n_levels, int order,
+                                               int pairs_mode, int n_list) {
+  PlainBwdPlan bp;
+  if (plan_plain_bwd(nX, LX, nY, LY, d, dtype, n_levels, order, pairs_mode, n_list, bp))
+    return 0;
+  return bp.pp.total;
+}
+
+int ksig_signature_kern_plain_bwd(const void* X, const int32_t* lenX, int nX, int LX,
+                                  const void* Y, const int32_t* lenY, int nY, int LY, int d,
+                                  int dtype, int static_kind, double static_param, int n_levels,
+                                  int order, int pairs_mode, const int32_t* pair_list,
+                                  int n_list, const double* grad_levels, void* dX,
+                                  double* dparam, void* workspace, size_t workspace_bytes,
+                                  void* stream) {
+  int rc = check_common(X, Y, pairs_mode, pair_list, n_list, static_kind, static_param);
+  if (rc) return rc;
+  if (!grad_levels || !dX) return fail(KSIG_ERR_INVALID, "grad_levels or dX is NULL");
+  PlainBwdPlan bp;
+  rc = plan_plain_bwd(nX, LX, nY, LY, d, dtype, n_levels, order, pairs_mode, n_list, bp);
+  if (rc) return rc;
+  if (!workspace || workspace_bytes < bp.pp.total)
+    return fail(KSIG_ERR_WORKSPACE, "workspace of %zu bytes is smaller than the %zu required",
+                workspace_bytes, bp.pp.total);
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  KSIG_CUDA(cudaMemsetAsync(workspace, 0, 16, st));
+  if (bp.pp.f.ntasks == 0) return KSIG_OK;
+  if (pairs_mode == KSIG_PAIRS_UPPER || pairs_mode == KSIG_PAIRS_DIAG) { nY = nX; LY = LX; Y = X; lenY = lenX; }
+  const int nl_out = n_levels;
+  if (dtype == KSIG_DTYPE_F64)
+    return run_plain_bwd<double>(bp, X, lenX, nX, LX, Y, lenY, nY, LY, d, 1, static_kind,
+                                 static_param, n_levels, pairs_mode, pair_list, grad_levels,
+                                 nl_out, dX, dparam, static_cast<char*>(workspace), st);
+  return run_plain_bwd<float>(bp, X, lenX, nX, LX, Y, lenY, nY, LY, d, 0, static_kind,
+                              static_param, n_levels, pairs_mode, pair_list, grad_levels, nl_out,
+                              dX, dparam, static_cast<char*>(workspace), st);
 }
 
 size_t ksig_signature_kern_bwd_workspace(int nX, int LX, int nY, int LY, int d, int dtype,

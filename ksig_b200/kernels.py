@@ -61,11 +61,18 @@ def _to_seqs(X, n_features, reset_obj=None):
         else torch.float64
     lens = [max(int(s.shape[0]), 1) for s in seqs]
     Lmax = max(lens)
+    lengths = torch.tensor(lens, dtype=torch.int32, device='cuda')
+    if any(s.requires_grad for s in seqs):
+      # Differentiable padding: gradients flow back to the list entries.
+      padded = torch.nn.utils.rnn.pad_sequence(
+          [s.to(device='cuda', dtype=dtype) if s.shape[0] > 0
+           else torch.zeros((1, d), dtype=dtype, device='cuda') for s in seqs],
+          batch_first=True)
+      return E.Seqs(padded.detach().contiguous(), lengths), False, padded
     data = torch.zeros((len(seqs), Lmax, d), dtype=dtype, device='cuda')
     for i, s in enumerate(seqs):
       if s.shape[0] > 0:
         data[i, :s.shape[0]] = s.to(device='cuda', dtype=dtype)
-    lengths = torch.tensor(lens, dtype=torch.int32, device='cuda')
     return E.Seqs(data, lengths), False, None
   was_torch = isinstance(X, torch.Tensor)
   if not was_torch:

@@ -142,3 +142,23 @@ def test_pde_grad_linear_multistrip_fp64():
          X, Y, 0.7, torch.float64, 1e-8)
   finally:
     del os.environ['KSIG_BWD_COLS']
+
+
+@pytest.mark.parametrize('dt,tol', [(torch.float64, 1e-9), (torch.float32, 1e-4)])
+@pytest.mark.parametrize('order,n_levels,kind', [(1, 5, 0), (2, 4, 0), (3, 4, 1)])
+def test_plain_bwd_baseline_matches_fused(dt, tol, order, n_levels, kind):
+  """The plain one-pair-per-block adjoint gives the fused adjoint's dX and
+  dparam on ragged inputs (the fused one is pinned to the oracle above)."""
+  from ksig_b200 import _engine as E
+  rng = np.random.default_rng(40 + order)
+  X = torch.tensor(_walks(rng, 3, 21, 3), dtype=dt, device='cuda')
+  Y = torch.tensor(_walks(rng, 4, 26, 3), dtype=dt, device='cuda')
+  lx = torch.tensor([21, 9, 15], dtype=torch.int32, device='cuda')
+  ly = torch.tensor([26, 4, 19, 11], dtype=torch.int32, device='cuda')
+  Xs, Ys = E.Seqs(X, lx), E.Seqs(Y, ly)
+  gl = torch.tensor(rng.standard_normal((n_levels + 1, 12)), device='cuda')
+  param = 0.9 if kind == 0 else 0.7
+  dXf, dpf = E.sig_levels_bwd(Xs, Ys, 0, n_levels, order, kind, param, gl)
+  dXp, dpp = E.sig_levels_bwd_plain(Xs, Ys, 0, n_levels, order, kind, param, gl)
+  assert _relerr(dXp, dXf) < tol
+  assert abs(dpp.item() - dpf.item()) <= tol * max(1.0, abs(dpf.item()))
