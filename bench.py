@@ -464,6 +464,85 @@ def run_ragged(args):
   print(json.dumps(line))
 
 
+# Ragged PDE workload (not the default bench line): N = M = 256 Brownian
+# paths (N(0, 1/L) increments, d = 3 plus a time channel), lengths uniform
+# in [64, 512], dyadic_order = 1, RBF bandwidth 1, normalize.  One call
+# through the public API, then the same call captured in a CUDA graph, then
+# replayed after the tile-width autotuner.
+
+def make_brownian(n, lmin, lmax, d, seed):
+  rng = np.random.default_rng(seed)
+  lens = rng.integers(lmin, lmax + 1, n)
+  data = np.zeros((n, lmax, d + 1), dtype=np.float32)
+  for i, L in enumerate(lens):
+    inc = rng.standard_normal((L - 1, d)) / np.sqrt(L)
+    data[i, 1:L, :d] = np.cumsum(inc, 0)
+    data[i, :L, d] = np.linspace(0, 1, L)
+  return data, lens
+
+
+def run_ragged_pde(args):
+  import torch
+
+  import ksig_b200 as K
+  from ksig_b200 import tuning
+  n = args.n_seq or 256
+  dev = torch.device('cuda', 0)
+  xd, lx = make_brownian(n, 64, 512, 3, 3)
+  yd, ly = make_brownian(n, 64, 512, 3, 4)
+  X = K.Ragged(torch.as_tensor(xd, device=dev), torch.as_tensor(lx, device=dev))
+  Y = K.Ragged(torch.as_tensor(yd, device=dev), torch.as_tensor(ly, device=dev))
+  kern = K.SignaturePDEKernel(dyadic_order=1, static_kernel=K.RBFKernel(1.0))
+  F = 2
+  cells = float(np.sum(lx - 1)) * float(np.sum(ly - 1)) * F * F
+
+  def timed(fn, steps, warm):
+    for _ in range(warm):
+      fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(steps):
+      a = torch.cuda.Event(enable_timing=True)
+      b = torch.cuda.Event(enable_timing=True)
+      a.record()
+      fn()
+      b.record()
+      b.synchronize()
+      ts.append(a.elapsed_time(b))
+    return sum(ts) / len(ts)
+
+  eager = timed(lambda: kern(X, Y, return_on_gpu=True), args.steps, args.warmup)
+  g = K.GraphedKernel(kern, X, Y)
+  graph = timed(g, args.steps, args.warmup)
+  tuned = tuning.autotune(kern, X, Y, reps=2)
+  gt = K.GraphedKernel(kern, X, Y)
+  graph_tuned = timed(gt, args.steps, args.warmup)
+  ref = kern(X, Y, return_on_gpu=True)
+  tuning.reset()
+  # FP32 against the FP64 path on a 16 x 16 corner.
+  c = min(16, n)
+  X64 = K.Ragged(X.data[:c].double(), X.lengths[:c])
+  Y64 = K.Ragged(Y.data[:c].double(), Y.lengths[:c])
+  k64 = kern(X64, Y64, return_on_gpu=True)
+  k32 = kern(K.Ragged(X.data[:c], X.lengths[:c]), K.Ragged(Y.data[:c], Y.lengths[:c]),
+             return_on_gpu=True)
+  rel = float(((k32.double() - k64).abs() / k64.abs().clamp_min(1e-300)).max())
+  line = {
+      'metric': METRIC, 'workload': f'sig_pde_rbf_ragged_N{n}_M{n}_L64-512_d4_dyadic1_normalized',
+      'unit': UNIT,
+      'eager': {'value': n * n / (eager * 1e-3), 'ms_per_step': eager},
+      'graph': {'value': n * n / (graph * 1e-3), 'ms_per_step': graph},
+      'graph_autotuned': {'value': n * n / (graph_tuned * 1e-3), 'ms_per_step': graph_tuned,
+                          'widths': {str(k): v[0] for k, v in tuned.items()}},
+      'refined_cells_per_s': cells / (min(graph, graph_tuned) * 1e-3),
+      'refined_cells': cells,
+      'rel_err_fp32_vs_fp64': rel,
+      'checksum': float(ref.double().sum()),
+      'steps': args.steps, 'warmup': args.warmup, 'dtype': 'f32', 'data': 'synthetic',
+  }
+  print(json.dumps(line))
+
+
 # ---------------------------------------------------------------------------
 # Reference arm: the reference recursion on the host cores.
 # ---------------------------------------------------------------------------
@@ -512,7 +591,8 @@ def main():
   ap.add_argument('--no-bwd', action='store_true')
   ap.add_argument('--no-plain', action='store_true')
   ap.add_argument('--bwd-steps', type=int, default=5)
-  ap.add_argument('--workload', default='dp512', choices=['dp512', 'ragged-dp'],
+  ap.add_argument('--workload', default='dp512',
+                  choices=['dp512', 'ragged-dp', 'ragged-pde'],
                   help='dp512: the bench line; ragged-dp: the 2048 x 2048 ragged '
                        'order-2 workload, printed as its own report line')
   ap.add_argument('--plain-sample', type=int, default=96)
@@ -541,6 +621,9 @@ def main():
     torch.cuda.set_device(0)
   if args.workload == 'ragged-dp':
     run_ragged(args)
+    return
+  if args.workload == 'ragged-pde':
+    run_ragged_pde(args)
     return
   try:
     run_ours(args, rank, world, dist)

@@ -287,6 +287,17 @@ int ksig_workspace_status(void* workspace, void* stream);
  *                        2 flops per FMA) with an FMA-chain kernel on `stream`
  *                        (synchronous).
  */
+/*
+ * Autotuning hook (no reference counterpart).  Sets the column count per
+ * lane (tile width) that later plans of one kernel family prefer:
+ * op 0 = DP forward, 1 = PDE forward, 2 = DP adjoint, 3 = PDE adjoint;
+ * cols 0 restores the built-in choice.  The nearest compiled width is used.
+ * Process-wide; the Python autotuner (ksig_b200.tuning) times the compiled
+ * widths on the caller's workload and sets the fastest.
+ */
+int ksig_tune_set_cols(int op, int cols);
+int ksig_tune_get_cols(int op);
+
 unsigned long long ksig_launch_count(void);
 void ksig_profile_enable(int on);
 int ksig_profile_read(double* total_ms, long long* launches);

@@ -4,10 +4,13 @@ Importing the package does not touch the GPU; the CUDA library
 (``lib/libksig_b200.so``) is loaded on first use.
 """
 
+from . import graphs  # noqa: F401
 from . import kernels  # noqa: F401
 from . import static  # noqa: F401
+from . import tuning  # noqa: F401
 from . import utils  # noqa: F401
-from .kernels import SignatureKernel, SignaturePDEKernel  # noqa: F401
+from .graphs import GraphedKernel  # noqa: F401
+from .kernels import Ragged, SignatureKernel, SignaturePDEKernel  # noqa: F401
 from .static.kernels import LinearKernel, RBFKernel  # noqa: F401
 
 __version__ = '0.1.0'

@@ -67,6 +67,8 @@ _SIGNATURES = {
     'ksig_signature_kern_plain_bwd': (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _I,
                                            _I, _I, _D, _I, _I, _I, _P, _I, _P,
                                            _P, _P, _P, _SZ, _P]),
+    'ksig_tune_set_cols': (_I, [_I, _I]),
+    'ksig_tune_get_cols': (_I, [_I]),
     'ksig_launch_count': (ctypes.c_ulonglong, []),
     'ksig_profile_enable': (None, [_I]),
     'ksig_profile_read': (_I, [ctypes.POINTER(ctypes.c_double),

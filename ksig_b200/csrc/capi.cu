@@ -19,6 +19,8 @@
 #include "pde_bwd.cuh"
 #include "plain.cuh"
 
+#include <cub/device/device_radix_sort.cuh>
+
 namespace ksig {
 namespace {
 
@@ -159,12 +161,16 @@ struct FwdPlan {
   int multi, grid, wpb;
   size_t dyn_smem;
   long long rows_max, scratch_per_warp, nwarps;
+  int ordered;            // workspace holds a longest-first task order
+  size_t sort_tmp;        // radix-sort temporary bytes
   size_t off_status, off_xr, off_yr, off_xstart, off_ystart, off_xlen, off_ylen,
-      off_scratch, total;
+      off_okeys, off_okeys2, off_ovals, off_order, off_sort, off_scratch, total;
   const KernelEntry* k;
 };
 
-// Workspace offsets of the packed points, lengths, starts and scratch.
+// Workspace offsets of the packed points, lengths, starts, the task-order
+// buffers and the per-warp scratch (last, so that the adjoint plans can
+// re-size it).
 void layout_fwd(FwdPlan& pl, int nX, int LX, int nY, int LY) {
   const size_t es = pl.f64 ? 8 : 4;
   size_t off = 0;
@@ -175,8 +181,85 @@ void layout_fwd(FwdPlan& pl, int nX, int LX, int nY, int LY) {
   pl.off_ystart = off; off = align_up(off + (size_t)nY * 8);
   pl.off_xlen = off; off = align_up(off + (size_t)nX * 4);
   pl.off_ylen = off; off = align_up(off + (size_t)nY * 4);
+  const size_t no = pl.ordered ? (size_t)pl.ntasks * 4 : 0;
+  pl.off_okeys = off; off = align_up(off + no);
+  pl.off_okeys2 = off; off = align_up(off + no);
+  pl.off_ovals = off; off = align_up(off + no);
+  pl.off_order = off; off = align_up(off + no);
+  pl.off_sort = off; off = align_up(off + (pl.ordered ? pl.sort_tmp : 0));
   pl.off_scratch = off; off = align_up(off + (size_t)pl.nwarps * pl.scratch_per_warp * es);
   pl.total = off;
+}
+
+int env_int(const char* name, int def);
+
+// ---- longest-first task order for ragged batches --------------------------
+// Pairs of a ragged batch differ in cost by up to the product of the length
+// ratios.  Sorting the task indices by cell count (descending) and handing
+// them out round-robin gives every warp one task of each cost band, so the
+// persistent grid drains evenly.  Tasks keep their output slots.
+
+__global__ void order_keys_kernel(int ntasks, int mode, int nY, const int2* list, int nX,
+                                  int nYseq, const int32_t* xlen, const int32_t* ylen, int diff,
+                                  uint32_t* keys, int32_t* vals) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntasks; t += gridDim.x * blockDim.x) {
+    const int2 ab = decode_task(t, mode, nY, list, nullptr);
+    uint32_t key = 0;
+    if (ab.x >= 0 && ab.x < nX && ab.y >= 0 && ab.y < nYseq) {
+      long long a = (long long)xlen[ab.x] - diff, b = (long long)ylen[ab.y] - diff;
+      a = a > 0 ? a : 0;
+      b = b > 0 ? b : 0;
+      const long long c = a * b;
+      key = c > 0xffffffffLL ? 0xffffffffu : (uint32_t)c;
+    }
+    keys[t] = key;
+    vals[t] = t;
+  }
+}
+
+// Decides whether a plan orders its tasks and sizes the sort temporary.
+void plan_order(FwdPlan& pl, int pairs_mode) {
+  pl.ordered = 0;
+  pl.sort_tmp = 0;
+  if (pairs_mode == KSIG_PAIRS_DIAG || pl.ntasks < 2048 || !env_int("KSIG_TASK_ORDER", 1)) return;
+  size_t bytes = 0;
+  cudaError_t e = cub::DeviceRadixSort::SortPairsDescending(
+      nullptr, bytes, (const uint32_t*)nullptr, (uint32_t*)nullptr, (const int32_t*)nullptr,
+      (int32_t*)nullptr, (int)pl.ntasks);
+  if (e != cudaSuccess) return;
+  pl.ordered = 1;
+  pl.sort_tmp = bytes;
+}
+
+// Builds the order in the workspace (after packing, which wrote the
+// lengths); null when the plan has no order or the batch is not ragged.
+const int* build_order(const FwdPlan& pl, bool ragged, int mode, int nY, const int32_t* list,
+                       int nX, int nYseq, char* ws, cudaStream_t st, int* rc) {
+  *rc = KSIG_OK;
+  if (!pl.ordered || !ragged) return nullptr;
+  uint32_t* k1 = reinterpret_cast<uint32_t*>(ws + pl.off_okeys);
+  uint32_t* k2 = reinterpret_cast<uint32_t*>(ws + pl.off_okeys2);
+  int32_t* v1 = reinterpret_cast<int32_t*>(ws + pl.off_ovals);
+  int32_t* v2 = reinterpret_cast<int32_t*>(ws + pl.off_order);
+  const int32_t* xl = reinterpret_cast<const int32_t*>(ws + pl.off_xlen);
+  const int32_t* yl = reinterpret_cast<const int32_t*>(ws + pl.off_ylen);
+  const int n = (int)pl.ntasks;
+  int blocks = (n + 255) / 256;
+  if (blocks > 4096) blocks = 4096;
+  order_keys_kernel<<<blocks, 256, 0, st>>>(n, mode, nY, reinterpret_cast<const int2*>(list), nX,
+                                            nYseq, xl, yl, pl.diff, k1, v1);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) {
+    size_t tmp = pl.sort_tmp;
+    e = cub::DeviceRadixSort::SortPairsDescending(ws + pl.off_sort, tmp, k1, k2, v1, v2, n, 0, 32,
+                                                  st);
+  }
+  if (e != cudaSuccess) {
+    *rc = cuda_fail(e, "task order");
+    return nullptr;
+  }
+  g_launches.fetch_add(2, std::memory_order_relaxed);
+  return v2;
 }
 
 long long num_pairs(int mode, int nX, int nY, int n_list) {
@@ -199,7 +282,14 @@ int env_int(const char* name, int def) {
 // Column count per lane: smallest c whose strip covers the longest column
 // sequence in one strip, capped by what the register budget allows.
 // KSIG_FWD_COLS overrides the choice (tuning).
-int want_cols(int ly_cells, int cap) {
+// Column counts chosen by the autotuner per kernel family (0: heuristic).
+std::atomic<int> g_tuned_cols[4];
+
+int tuned_cols(int op) { return (op >= 0 && op < 4) ? g_tuned_cols[op].load() : 0; }
+
+int want_cols(int ly_cells, int cap, int op) {
+  const int tuned = tuned_cols(op);
+  if (tuned > 0) return tuned;
   const int forced = env_int("KSIG_FWD_COLS", 0);
   if (forced > 0) return forced;
   static const int opts[] = {2, 4, 7, 8};
@@ -212,7 +302,7 @@ int want_cols(int ly_cells, int cap) {
 
 int plan_fwd(bool pde, int nX, int LX, int nY, int LY, int d, int dtype, int n_levels,
              int order_or_dyadic, int difference, int pairs_mode, int n_list,
-             FwdPlan& pl) {
+             FwdPlan& pl, bool allow_order = true) {
   if (dtype != KSIG_DTYPE_F32 && dtype != KSIG_DTYPE_F64)
     return fail(KSIG_ERR_INVALID, "dtype must be KSIG_DTYPE_F32 or KSIG_DTYPE_F64");
   if (nX <= 0 || LX <= 0 || d <= 0) return fail(KSIG_ERR_INVALID, "empty X (n=%d, L=%d, d=%d)", nX, LX, d);
@@ -241,7 +331,7 @@ int plan_fwd(bool pde, int nX, int LX, int nY, int LY, int d, int dtype, int n_l
   const int ly_cells = pl.diff ? LY - 1 : LY;
   const int lx_cells = pl.diff ? LX - 1 : LX;
   const int op = pde ? OP_PDE_FWD : OP_DP_FWD;
-  const int want = want_cols(ly_cells, 8);
+  const int want = want_cols(ly_cells, 8, op);
   const KernelEntry* k = find_kernel(op, pl.f64, d, want, need_nl, p, pl.diff);
   if (!k)
     return fail(KSIG_ERR_UNSUPPORTED,
@@ -280,6 +370,7 @@ int plan_fwd(bool pde, int nX, int LX, int nY, int LY, int d, int dtype, int n_l
   pl.rows_max = lx_cells > 32 ? lx_cells : 32;
   pl.scratch_per_warp = pl.multi ? pl.rows_max * pl.nx_exchange : 0;
   pl.nwarps = nwarps;
+  if (allow_order) plan_order(pl, pairs_mode);
   layout_fwd(pl, nX, LX, nY, LY);
   return KSIG_OK;
 }
@@ -336,7 +427,9 @@ int run_fwd(const FwdPlan& pl, const void* X, const int32_t* lenX, int nX, int L
   a.mode = mode;
   a.nY = self ? nX : nY;
   a.list = reinterpret_cast<const int2*>(list);
-  a.order = nullptr;
+  a.order = build_order(pl, lenX || lenY, mode, self ? nX : nY, list, nX, self ? nX : nY, ws, st,
+                        &rc);
+  if (rc) return rc;
   a.ntasks = (int)pl.ntasks;
   a.kind = kind;
   a.out = out;
@@ -374,7 +467,8 @@ int plan_bwd(int nX, int LX, int nY, int LY, int d, int dtype, int n_levels, int
   const int ly = LY - 1, lx = LX - 1;
   // Column count: fewest lane-steps per row, ns(C) * C, over the compiled
   // variants (ties go to the wider strip: fewer strips, fewer records).
-  const int forced = env_int("KSIG_BWD_COLS", 0);
+  const int forced = tuned_cols(OP_DP_BWD) > 0 ? tuned_cols(OP_DP_BWD)
+                                              : env_int("KSIG_BWD_COLS", 0);
   const KernelEntry* k = nullptr;
   long long best_cost = -1;
   for (int want : {8, 7, 6, 5, 4, 3, 2, 1}) {
@@ -448,7 +542,9 @@ int run_bwd(const BwdPlan& bp, const void* X, const int32_t* lenX, int nX, int L
   a.mode = mode;
   a.nY = self ? nX : nY;
   a.list = reinterpret_cast<const int2*>(list);
-  a.order = nullptr;
+  a.order = build_order(pl, lenX || lenY, mode, self ? nX : nY, list, nX, self ? nX : nY, ws, st,
+                        &rc);
+  if (rc) return rc;
   a.ntasks = (int)pl.ntasks;
   a.nX = nX;
   a.nYseq = self ? nX : nY;
@@ -490,7 +586,8 @@ int plan_pde_bwd(int nX, int LX, int nY, int LY, int d, int dtype, int dyadic, i
   if (pairs_mode == KSIG_PAIRS_UPPER || pairs_mode == KSIG_PAIRS_DIAG) { nY = nX; LY = LX; }
   const int ly = LY - 1, lx = LX - 1;
   bp.F = 1 << dyadic;
-  const int forced = env_int("KSIG_BWD_COLS", 0);
+  const int forced = tuned_cols(OP_PDE_BWD) > 0 ? tuned_cols(OP_PDE_BWD)
+                                               : env_int("KSIG_BWD_COLS", 0);
   const int want = forced > 0 ? forced : (ly <= 63 ? 2 : (ly <= 127 ? 4 : 8));
   const KernelEntry* k = find_kernel(OP_PDE_BWD, bp.f.f64, d, want, 0, bp.F, 1);
   if (!k)
@@ -548,6 +645,9 @@ int run_pde_bwd(const PdeBwdPlan& bp, const void* X, const int32_t* lenX, int nX
   a.mode = mode;
   a.nY = self ? nX : nY;
   a.list = reinterpret_cast<const int2*>(list);
+  a.order = build_order(pl, lenX || lenY, mode, self ? nX : nY, list, nX, self ? nX : nY, ws, st,
+                        &rc);
+  if (rc) return rc;
   a.ntasks = (int)pl.ntasks;
   a.nX = nX;
   a.nYseq = self ? nX : nY;
@@ -735,13 +835,13 @@ int fwd_entry(bool pde, const void* X, const int32_t* lenX, int nX, int LX, cons
               const int32_t* lenY, int nY, int LY, int d, int dtype, int static_kind,
               double static_param, int n_levels, int order_or_dyadic, int difference,
               int pairs_mode, const int32_t* list, int n_list, double* out, void* ws,
-              size_t ws_bytes, void* stream) {
+              size_t ws_bytes, void* stream, bool allow_order = true) {
   int rc = check_common(X, Y, pairs_mode, list, n_list, static_kind, static_param);
   if (rc) return rc;
   if (!out) return fail(KSIG_ERR_INVALID, "output is NULL");
   FwdPlan pl;
   rc = plan_fwd(pde, nX, LX, nY, LY, d, dtype, n_levels, order_or_dyadic, difference, pairs_mode,
-                n_list, pl);
+                n_list, pl, allow_order);
   if (rc) return rc;
   if (!ws || ws_bytes < pl.total)
     return fail(KSIG_ERR_WORKSPACE, "workspace of %zu bytes is smaller than the %zu required",
@@ -883,9 +983,10 @@ int ksig_signature_kern_static(const void* X, const int32_t* lenX, int nX, int L
                                void* stream) {
   int rc = check_common(X, Y, pairs_mode, pair_list, n_list, static_kind, static_param);
   if (rc) return rc;
+  // The fixed scratch holds no task-order buffers: tasks run in natural order.
   FwdPlan pl;
   rc = plan_fwd(false, nX, LX, nY, LY, d, dtype, n_levels, order, difference, pairs_mode,
-                n_list, pl);
+                n_list, pl, false);
   if (rc) return rc;
   if (pl.total > kStaticScratchBytes)
     return fail(KSIG_ERR_WORKSPACE,
@@ -897,7 +998,7 @@ int ksig_signature_kern_static(const void* X, const int32_t* lenX, int nX, int L
   if (!ws) return cuda_fail(e, "cudaGetSymbolAddress(g_static_scratch)");
   return fwd_entry(false, X, lenX, nX, LX, Y, lenY, nY, LY, d, dtype, static_kind, static_param,
                    n_levels, order, difference, pairs_mode, pair_list, n_list, out_levels, ws,
-                   kStaticScratchBytes, stream);
+                   kStaticScratchBytes, stream, false);
 }
 
 size_t ksig_signature_kern_plain_workspace(int nX, int LX, int nY, int LY, int d, int dtype,
@@ -1104,6 +1205,15 @@ int ksig_profile_read(double* total_ms, long long* launches) {
   if (launches) *launches = (long long)ev.size();
   return KSIG_OK;
 }
+
+int ksig_tune_set_cols(int op, int cols) {
+  if (op < 0 || op > 3) return fail(KSIG_ERR_INVALID, "bad kernel family %d", op);
+  if (cols < 0 || cols > 32) return fail(KSIG_ERR_INVALID, "bad column count %d", cols);
+  g_tuned_cols[op].store(cols);
+  return KSIG_OK;
+}
+
+int ksig_tune_get_cols(int op) { return tuned_cols(op); }
 
 int ksig_fp32_peak(double* tflops, void* stream) {
   if (!tflops) return fail(KSIG_ERR_INVALID, "NULL output");

@@ -42,6 +42,7 @@ struct PdeBwdArgs {
   const int32_t* ylen;
   int mode, nY;
   const int2* list;
+  const int* order;       // optional task permutation (longest first)
   int ntasks, nX, nYseq;
   int kind;
   double param;
@@ -77,7 +78,8 @@ pde_bwd_kernel(const PdeBwdArgs<T> args) {
   const bool rbf = args.kind == KIND_RBF;
 
   for (long long tid = wg; tid < args.ntasks; tid += nw) {
-    const int2 ab = decode_task((int)tid, args.mode, args.nY, args.list, nullptr);
+    const int2 ab = decode_task((int)tid, args.mode, args.nY, args.list, args.order);
+    const int task = args.order ? args.order[tid] : (int)tid;
     if (ab.x < 0 || ab.x >= args.nX || ab.y < 0 || ab.y >= args.nYseq) {
       if (lane == 0) set_status(args.status, KSIG_ERR_INVALID);
       continue;
@@ -92,7 +94,7 @@ pde_bwd_kernel(const PdeBwdArgs<T> args) {
       continue;
     }
     const int N = lx * F, M = ly * F;
-    const T w = (T)args.grad[tid];
+    const T w = (T)args.grad[task];
     const T* xb = args.xr + args.xstart[a] * RS;
     const T* yb = args.yr + args.ystart[b] * RS;
 

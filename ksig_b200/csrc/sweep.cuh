@@ -101,7 +101,7 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
       it.xb = args.xr;
       return;
     }
-    it.task = (int)tid;
+    it.task = args.order ? args.order[tid] : (int)tid;
     int2 ab = decode_task((int)tid, args.mode, args.nY, args.list, args.order);
     if (ab.x < 0 || ab.x >= args.nX || ab.y < 0 || ab.y >= args.nYseq) {
       set_status(args.status, KSIG_ERR_INVALID);  // pair index out of range

@@ -34,6 +34,33 @@ from . import utils
 from .static.kernels import StaticKernel
 
 
+class Ragged:
+  """A ragged batch as one dense padded tensor plus per-sequence lengths.
+
+  ``data`` is ``[n, L, d]`` (points past ``lengths[i]`` are ignored, which
+  equals the reference on the edge-padded array) and ``lengths`` ``[n]``.
+  Unlike a Python list it costs no per-sequence copies, keeps fixed device
+  buffers (so a call on it can be captured in a CUDA graph) and, when
+  ``data`` requires grad, takes gradients directly.  No reference
+  counterpart.
+  """
+
+  __slots__ = ('data', 'lengths')
+
+  def __init__(self, data, lengths):
+    data = torch.as_tensor(data)
+    lengths = torch.as_tensor(lengths)
+    if data.ndim != 3:
+      raise ValueError('Ragged data must be [n, L, d]')
+    if lengths.ndim != 1 or lengths.shape[0] != data.shape[0]:
+      raise ValueError('Ragged lengths must be [n]')
+    self.data = data
+    self.lengths = lengths
+
+  def __len__(self):
+    return self.data.shape[0]
+
+
 def _is_ragged(X):
   return isinstance(X, (list, tuple))
 
@@ -45,6 +72,24 @@ def _to_seqs(X, n_features, reset_obj=None):
   inputs; ragged inputs (lists) are padded and carry their lengths.
   Returns (Seqs, was_torch, requires_grad_tensor_or_None).
   """
+  if isinstance(X, Ragged):
+    data = X.data
+    if n_features is not None and data.shape[-1] != n_features:
+      raise ValueError(
+          'Number of features in `X` does not match saved `n_features` param.')
+    if data.dtype not in (torch.float32, torch.float64):
+      data = data.to(torch.float64)
+    lengths = X.lengths.to(device='cuda', dtype=torch.int32)
+    # Host-side range check, skipped while a CUDA graph is being captured
+    # (it would synchronise); the packing kernel checks the lengths on the
+    # device as well.
+    if (not torch.cuda.is_current_stream_capturing() and int(lengths.numel()) and
+        (bool((lengths < 0).any()) or bool((lengths > data.shape[1]).any()))):
+      raise ValueError('Ragged lengths must lie in [0, L]')
+    lengths = lengths.clamp_min(1)
+    grad_src = data if data.requires_grad else None
+    Xd = data.detach().to('cuda').contiguous()
+    return E.Seqs(Xd, lengths), False, grad_src
   if _is_ragged(X):
     seqs = [s if isinstance(s, torch.Tensor) else torch.as_tensor(np.asarray(s))
             for s in X]
