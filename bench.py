@@ -543,6 +543,103 @@ def run_ragged_pde(args):
   print(json.dumps(line))
 
 
+# MMD^2 gradient workload (not the default bench line): 128 'generated' and
+# 128 'target' Brownian paths with per-path drift ~ N(0, 0.5), L = 128,
+# d = 4, SignaturePDEKernel(dyadic_order=2), RBF bandwidth 1.  Times
+# MMD^2 = mean K(X,X) + mean K(Y,Y) - 2 mean K(X,Y) and its gradient with
+# respect to X and the bandwidth (FP32), and checks the FP64 gradient against
+# central finite differences (h = 1e-6) on 16 random coordinates.
+
+def make_drift_paths(n, L, d, seed):
+  rng = np.random.default_rng(seed)
+  drift = rng.standard_normal((n, 1, d)) * np.sqrt(0.5)
+  inc = rng.standard_normal((n, L - 1, d)) / np.sqrt(L) + drift / L
+  return np.concatenate([np.zeros((n, 1, d)), np.cumsum(inc, 1)], 1)
+
+
+def run_mmd_pde(args):
+  import torch
+
+  import ksig_b200 as K
+  n = args.n_seq or 128
+  dev = torch.device('cuda', 0)
+  Xn = make_drift_paths(n, 128, 4, 41)
+  Yn = make_drift_paths(n, 128, 4, 42)
+
+  def mmd2(kern, X, Y):
+    return (kern(X, return_on_gpu=True).mean() + kern(Y, return_on_gpu=True).mean()
+            - 2.0 * kern(X, Y, return_on_gpu=True).mean())
+
+  def timed(fn, steps, warm):
+    for _ in range(warm):
+      fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(steps):
+      a = torch.cuda.Event(enable_timing=True)
+      b = torch.cuda.Event(enable_timing=True)
+      a.record()
+      fn()
+      b.record()
+      b.synchronize()
+      ts.append(a.elapsed_time(b))
+    return sum(ts) / len(ts)
+
+  X32 = torch.tensor(Xn, dtype=torch.float32, device=dev, requires_grad=True)
+  Y32 = torch.tensor(Yn, dtype=torch.float32, device=dev)
+  bw = torch.tensor(1.0, dtype=torch.float64, requires_grad=True)
+  kern = K.SignaturePDEKernel(dyadic_order=2, static_kernel=K.RBFKernel(bw))
+
+  def fwd():
+    with torch.no_grad():
+      mmd2(kern, X32, Y32)
+
+  def fb():
+    X32.grad = None
+    bw.grad = None
+    mmd2(kern, X32, Y32).backward()
+
+  fwd_ms = timed(fwd, args.steps, args.warmup)
+  fb_ms = timed(fb, args.steps, args.warmup)
+  if args.no_cpu:  # skip the finite-difference check (profiling runs)
+    fd = None
+  else:
+    X64 = torch.tensor(Xn, dtype=torch.float64, device=dev, requires_grad=True)
+    Y64 = torch.tensor(Yn, dtype=torch.float64, device=dev)
+    b64 = torch.tensor(1.0, dtype=torch.float64, requires_grad=True)
+    mmd2(K.SignaturePDEKernel(dyadic_order=2, static_kernel=K.RBFKernel(b64)),
+         X64, Y64).backward()
+    gX = X64.grad.cpu().numpy()
+
+    def f(Xv, b):
+      k = K.SignaturePDEKernel(dyadic_order=2, static_kernel=K.RBFKernel(b))
+      with torch.no_grad():
+        return float(mmd2(k, torch.tensor(Xv, device=dev), Y64))
+
+    rng = np.random.default_rng(7)
+    h = 1e-6
+    errs = []
+    for _ in range(16):
+      i = tuple(int(rng.integers(0, s)) for s in Xn.shape)
+      Xp, Xm = Xn.copy(), Xn.copy()
+      Xp[i] += h
+      Xm[i] -= h
+      d_fd = (f(Xp, 1.0) - f(Xm, 1.0)) / (2 * h)
+      errs.append(abs(d_fd - gX[i]) / max(np.abs(gX).max(), 1e-300))
+    fdb = (f(Xn, 1.0 + h) - f(Xn, 1.0 - h)) / (2 * h)
+    fd = {'coords': 16, 'h': h, 'max_rel_err_dX': float(max(errs)),
+          'dbandwidth': float(b64.grad), 'dbandwidth_fd': fdb,
+          'rel_err_dbandwidth': abs(fdb - float(b64.grad)) / max(1.0, abs(fdb))}
+  line = {
+      'metric': METRIC, 'workload': f'mmd2_sig_pde_rbf_N{n}_M{n}_L128_d4_dyadic2',
+      'forward_ms': fwd_ms, 'fwd_bwd': {'s_per_step': fb_ms * 1e-3, 'ms_per_step': fb_ms,
+                                        'what': 'MMD^2 and d/dX, d/dbandwidth (FP32)'},
+      'fd_check_fp64': fd,
+      'steps': args.steps, 'warmup': args.warmup, 'dtype': 'f32', 'data': 'synthetic',
+  }
+  print(json.dumps(line))
+
+
 # ---------------------------------------------------------------------------
 # Reference arm: the reference recursion on the host cores.
 # ---------------------------------------------------------------------------
@@ -592,7 +689,7 @@ def main():
   ap.add_argument('--no-plain', action='store_true')
   ap.add_argument('--bwd-steps', type=int, default=5)
   ap.add_argument('--workload', default='dp512',
-                  choices=['dp512', 'ragged-dp', 'ragged-pde'],
+                  choices=['dp512', 'ragged-dp', 'ragged-pde', 'mmd-pde'],
                   help='dp512: the bench line; ragged-dp: the 2048 x 2048 ragged '
                        'order-2 workload, printed as its own report line')
   ap.add_argument('--plain-sample', type=int, default=96)
@@ -624,6 +721,9 @@ def main():
     return
   if args.workload == 'ragged-pde':
     run_ragged_pde(args)
+    return
+  if args.workload == 'mmd-pde':
+    run_mmd_pde(args)
     return
   try:
     run_ours(args, rank, world, dist)

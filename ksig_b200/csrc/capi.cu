@@ -601,7 +601,8 @@ int plan_pde_bwd(int nX, int LX, int nY, int LY, int d, int dtype, int dyadic, i
   const long long Mref = (long long)(ly > 1 ? ly : 1) * bp.F;
   bp.grid_stride = (Mref + 3) / 4 * 4;
   bp.bb_off = Nref * bp.grid_stride;
-  bp.scratch_per_warp = bp.bb_off + (long long)bp.rows_max * (2 * bp.F + 2);
+  // Multiple of 4 elements: every warp's adjoint grid starts 16-byte aligned.
+  bp.scratch_per_warp = (bp.bb_off + (long long)bp.rows_max * (2 * bp.F + 2) + 3) / 4 * 4;
   const size_t es = bp.f.f64 ? 8 : 4;
   int occ = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k->func, k->wpb * 32, 0);

@@ -58,9 +58,24 @@ struct PdeBwdArgs {
   int* status;
 };
 
+// W-wide vector of T (W * sizeof(T) <= 16) for the adjoint-grid traffic.
+template <typename T, int W> struct VecW;
+template <> struct VecW<float, 1> { using type = float; };
+template <> struct VecW<float, 2> { using type = float2; };
+template <> struct VecW<float, 4> { using type = float4; };
+template <> struct VecW<double, 1> { using type = double; };
+template <> struct VecW<double, 2> { using type = double2; };
+
 template <typename T, int KD, int C, int F, int WPB>
 __global__ void __launch_bounds__(WPB * 32)
 pde_bwd_kernel(const PdeBwdArgs<T> args) {
+  // A lane's F refined columns of one cell are contiguous in G (reversed in
+  // phase 2), so they move as W-wide vectors: the grid row base and the
+  // per-warp scratch are 16-byte aligned and F * (cell column) is a
+  // multiple of W.
+  constexpr int GW0 = 16 / (int)sizeof(T);
+  constexpr int GW = F < GW0 ? F : GW0;
+  using GV = typename VecW<T, GW>::type;
   constexpr int RS = packed_stride<T>(KD);
   constexpr int VN = Vec<T>::N;
   using V = typename Vec<T>::type;
@@ -216,9 +231,15 @@ pde_bwd_kernel(const PdeBwdArgs<T> args) {
             for (int c = 0; c < C; ++c) {
               const bool valid = g0 + c < ly && !(lane == 31 && c == C - 1);
               if (valid) {
+                GV* dst = reinterpret_cast<GV*>(Gs + grow * GS + (long long)(g0 + c) * F);
 #pragma unroll
-                for (int g = 0; g < F; ++g)
-                  Gs[grow * GS + (long long)(g0 + c) * F + g] = Kr[c * F + g];
+                for (int v = 0; v < F / GW; ++v) {
+                  GV gv;
+                  T* e = reinterpret_cast<T*>(&gv);
+#pragma unroll
+                  for (int i = 0; i < GW; ++i) e[i] = Kr[c * F + v * GW + i];
+                  __stcg(dst + v, gv);
+                }
               }
             }
           }
@@ -303,6 +324,23 @@ pde_bwd_kernel(const PdeBwdArgs<T> args) {
               for (int c = 0; c < C; ++c) {
                 const bool skip = (c == C - 1) && lane == 31;
                 const bool valid = g0 + c < ly && !skip;
+                // Lam of the cell's F refined columns: G columns
+                // M - (g0+c+1)F .. M - (g0+c)F - 1, in reverse.
+                T lamv[F];
+                if (valid) {
+                  const GV* src = reinterpret_cast<const GV*>(
+                      Gs + grow * GS + (long long)(M - (g0 + c + 1) * F));
+#pragma unroll
+                  for (int v = 0; v < F / GW; ++v) {
+                    const GV gv = __ldcg(src + v);
+                    const T* e = reinterpret_cast<const T*>(&gv);
+#pragma unroll
+                    for (int i = 0; i < GW; ++i) lamv[F - 1 - (v * GW + i)] = e[i];
+                  }
+                } else {
+#pragma unroll
+                  for (int g = 0; g < F; ++g) lamv[g] = T(0);
+                }
 #pragma unroll
                 for (int g = 0; g < F; ++g) {
                   const int J = c * F + g;
@@ -311,8 +349,7 @@ pde_bwd_kernel(const PdeBwdArgs<T> args) {
                   const T Hn = H + gg;
                   const T krn = kro + Hn;
                   if (valid) {
-                    const long long gcol = (long long)(M - 1 - ((g0 + c) * F + g));
-                    const T lam = __ldcg(Gs + grow * GS + gcol);
+                    const T lam = lamv[g];
                     const T q6 = qv[c] * (T(1) / T(6));
                     Zb[c] = fma(lam, fma(kro + kln, T(0.5) + q6, klo * q6), Zb[c]);
                   }
