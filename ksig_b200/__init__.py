@@ -13,4 +13,6 @@ from .graphs import GraphedKernel  # noqa: F401
 from .kernels import Ragged, SignatureKernel, SignaturePDEKernel  # noqa: F401
 from .static.kernels import LinearKernel, RBFKernel  # noqa: F401
 
+from ._engine import check_device_status  # noqa: F401
+
 __version__ = '0.1.0'

@@ -32,6 +32,37 @@ def _workspace(nbytes, device):
   return torch.empty(max(int(nbytes), 16), dtype=torch.uint8, device=device)
 
 
+# Device-side checks (lengths outside [1, L], pair indices out of range,
+# scratch geometry) never trap: the kernels record a status code in the
+# first word of the call's workspace.  Every call folds that word into a
+# per-device accumulator on the stream, without synchronising;
+# check_device_status() reads and clears it at a point that synchronises
+# anyway (the NumPy return of a kernel call) or when the caller asks.
+_STATUS = {}
+
+
+def _fold_status(ws):
+  idx = ws.device.index if ws.device.index is not None else torch.cuda.current_device()
+  acc = _STATUS.get(idx)
+  if acc is None:
+    acc = _STATUS[idx] = torch.zeros((1,), dtype=torch.int32, device=ws.device)
+  torch.maximum(acc, ws[:4].view(torch.int32), out=acc)
+
+
+def check_device_status():
+  """Synchronises, then raises if a call since the last check recorded a
+  device-side error: ValueError for invalid inputs (the reference's
+  exception type), KsigError otherwise.  Clears the record."""
+  for acc in _STATUS.values():
+    code = int(acc.item())
+    if code:
+      acc.zero_()
+      if code == L.ERR_INVALID:
+        raise ValueError('device-side check failed: a sequence length is '
+                         'outside [1, L] or a pair index is out of range')
+      raise L.KsigError(code, f'device-side check failed (code {code})')
+
+
 class Seqs:
   """A batch of sequences on the device: dense ``[n, L, d]`` plus lengths."""
 
@@ -78,6 +109,7 @@ def sig_levels(X, Y, mode, n_levels, order, difference, kind, param,
       order, int(difference), mode, _ptr(pair_list), n_list, _ptr(out),
       _ptr(ws), ws_bytes, _stream())
   L.check(rc)
+  _fold_status(ws)
   return out
 
 
@@ -100,6 +132,7 @@ def sig_levels_plain(X, Y, mode, n_levels, order, kind, param):
       _ptr(Yv.lengths), Yv.n, Yv.L, X.d, dt, kind, float(param), n_levels,
       order, mode, None, 0, _ptr(out), _ptr(ws), ws_bytes, _stream())
   L.check(rc)
+  _fold_status(ws)
   return out
 
 
@@ -132,6 +165,7 @@ def sig_levels_bwd(X, Y, mode, n_levels, order, kind, param, grad_levels,
       order, 1, mode, _ptr(pair_list), n_list, _ptr(gl), _ptr(dX),
       _ptr(dpar), _ptr(ws), ws_bytes, _stream())
   L.check(rc)
+  _fold_status(ws)
   return dX, dpar
 
 
@@ -159,6 +193,7 @@ def sig_levels_bwd_plain(X, Y, mode, n_levels, order, kind, param, grad_levels,
       order, mode, None, 0, _ptr(gl), _ptr(dX), _ptr(dpar), _ptr(ws),
       ws_bytes, _stream())
   L.check(rc)
+  _fold_status(ws)
   return dX, dpar
 
 
@@ -188,6 +223,7 @@ def pde_values(X, Y, mode, dyadic_order, difference, kind, param,
       dyadic_order, int(difference), mode, _ptr(pair_list), n_list,
       _ptr(out), _ptr(ws), ws_bytes, _stream())
   L.check(rc)
+  _fold_status(ws)
   return out
 
 
@@ -236,4 +272,5 @@ def pde_values_bwd(X, Y, mode, dyadic_order, kind, param, grad, dX=None,
       dyadic_order, 1, mode, _ptr(pair_list), n_list, _ptr(g), _ptr(dX),
       _ptr(dpar), _ptr(ws), ws_bytes, _stream())
   L.check(rc)
+  _fold_status(ws)
   return dX, dpar

@@ -572,8 +572,8 @@ int run_bwd(const BwdPlan& bp, const void* X, const int32_t* lenX, int nX, int L
 struct PdeBwdPlan {
   FwdPlan f;
   const KernelEntry* k;
-  int c, F, grid, rows_max;
-  long long grid_stride, bb_off, scratch_per_warp;
+  int c, F, grid, rows_max, ns_max;
+  long long scratch_per_warp;
   size_t off_scratch, total;
 };
 
@@ -586,10 +586,22 @@ int plan_pde_bwd(int nX, int LX, int nY, int LY, int d, int dtype, int dyadic, i
   if (pairs_mode == KSIG_PAIRS_UPPER || pairs_mode == KSIG_PAIRS_DIAG) { nY = nX; LY = LX; }
   const int ly = LY - 1, lx = LX - 1;
   bp.F = 1 << dyadic;
+  // Column count: fewest lane-steps per row, ns(C) * C, over the compiled
+  // variants (ties go to the wider strip: fewer strips, fewer records).
   const int forced = tuned_cols(OP_PDE_BWD) > 0 ? tuned_cols(OP_PDE_BWD)
                                                : env_int("KSIG_BWD_COLS", 0);
-  const int want = forced > 0 ? forced : (ly <= 63 ? 2 : (ly <= 127 ? 4 : 8));
-  const KernelEntry* k = find_kernel(OP_PDE_BWD, bp.f.f64, d, want, 0, bp.F, 1);
+  const KernelEntry* k = nullptr;
+  long long best_cost = -1;
+  for (int want : {8, 4, 2, 1}) {
+    if (forced > 0 && want != forced) continue;
+    const KernelEntry* e = find_kernel(OP_PDE_BWD, bp.f.f64, d, want, 0, bp.F, 1);
+    if (!e || e->c != want) continue;
+    const int strip = 32 * e->c - 1;
+    const long long ns = ly <= strip ? 1 : (ly + strip - 1) / strip;
+    const long long cost = ns * e->c;
+    if (best_cost < 0 || cost < best_cost) { best_cost = cost; k = e; }
+  }
+  if (!k && forced > 0) k = find_kernel(OP_PDE_BWD, bp.f.f64, d, forced, 0, bp.F, 1);
   if (!k)
     return fail(KSIG_ERR_UNSUPPORTED, "no compiled PDE backward kernel for dtype=%s d=%d "
                 "dyadic_order=%d", bp.f.f64 ? "f64" : "f32", d, dyadic);
@@ -597,20 +609,17 @@ int plan_pde_bwd(int nX, int LX, int nY, int LY, int d, int dtype, int dyadic, i
   bp.c = k->c;
   repack_for(bp.f, k->kd, nX, LX, nY, LY);
   bp.rows_max = lx > 1 ? lx : 1;
-  const long long Nref = (long long)(lx > 1 ? lx : 1) * bp.F;
-  const long long Mref = (long long)(ly > 1 ? ly : 1) * bp.F;
-  bp.grid_stride = (Mref + 3) / 4 * 4;
-  bp.bb_off = Nref * bp.grid_stride;
-  // Multiple of 4 elements: every warp's adjoint grid starts 16-byte aligned.
-  bp.scratch_per_warp = (bp.bb_off + (long long)bp.rows_max * (2 * bp.F + 2) + 3) / 4 * 4;
+  const int strip = 32 * bp.c - 1;
+  bp.ns_max = ly <= strip ? 1 : (ly + strip - 1) / strip;
+  bp.scratch_per_warp = (pde_bwd_scratch_elems(bp.ns_max, bp.rows_max, bp.c, bp.F) + 3) / 4 * 4;
   const size_t es = bp.f.f64 ? 8 : 4;
   int occ = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k->func, k->wpb * 32, 0);
   if (e != cudaSuccess || occ <= 0) occ = 1;
   const int sms = sm_count() > 0 ? sm_count() : 148;
   long long warps = (long long)sms * occ * k->wpb;
-  // Keep the adjoint grids within a few GB of scratch.
-  const long long budget = (long long)env_int("KSIG_PDE_BWD_SCRATCH_MB", 4096) << 20;
+  // The K records grow with rows x strips; keep the scratch within a budget.
+  const long long budget = (long long)env_int("KSIG_PDE_BWD_SCRATCH_MB", 16384) << 20;
   const long long cap = budget / (long long)(bp.scratch_per_warp * es);
   if (warps > cap) warps = cap > (long long)k->wpb ? cap : k->wpb;
   if (warps > bp.f.ntasks) warps = bp.f.ntasks > 0 ? bp.f.ntasks : 1;
@@ -661,8 +670,7 @@ int run_pde_bwd(const PdeBwdPlan& bp, const void* X, const int32_t* lenX, int nX
   a.dparam = dparam;
   a.scratch = reinterpret_cast<T*>(ws + bp.off_scratch);
   a.scratch_per_warp = bp.scratch_per_warp;
-  a.grid_stride = bp.grid_stride;
-  a.bb_off = bp.bb_off;
+  a.ns_max = bp.ns_max;
   a.rows_max = bp.rows_max;
   a.status = status;
   void* kargs[] = {&a};

@@ -4,28 +4,33 @@
 // Forward scheme per refined cell (ksig/algorithms.py:384-385, q = Z / F^2):
 //   K[i+1,j+1] = A (K[i,j+1] + K[i+1,j]) - B K[i,j],
 //   A = 1 + q/2 + q^2/12, B = 1 - q^2/12, output K[N, M].
-// Exact discrete adjoint: with L = w K[N, M], Lam = dL/dK satisfies
-//   Lam[i,j] = A(i,j-1) Lam[i+1,j] + A(i-1,j) Lam[i,j+1] - B(i,j) Lam[i+1,j+1]
-// (coefficients of the refined cell named; cells outside the grid give 0),
-// Lam[N,M] = w, and
-//   dL/dq(i,j) = Lam[i+1,j+1] ((K[i,j+1] + K[i+1,j]) (1/2 + q/6) + K[i,j] q/6).
-// On the grid reversed in both axes, G(a,b) = Lam[N-a, M-b] obeys a
-// forward-type scheme
-//   G(a,b) = Ar G(a-1,b) + Ab G(a,b-1) - B G(a-1,b-1)
-// whose B comes from the point's own (reversed) cell and whose Ar / Ab come
-// from the cells above and to the left of it, with zero boundaries and the
-// seed G(0,0) = w.  Both passes therefore run as the forward kernel does:
-// lanes own column blocks, lane l one row step behind lane l-1, and the
-// update in increment form (H = vertical increment accumulated along the
-// row) that keeps FP32 rounding small.
+// Exact discrete adjoint: with L = w K[N, M] and G(i,j) = dL/dK[i+1,j+1]
+// (the adjoint of a refined cell's lower-right corner),
+//   G(i,j) = A(i+1,j) G(i+1,j) + A(i,j+1) G(i,j+1) - B(i+1,j+1) G(i+1,j+1)
+// (cells outside the grid contribute nothing), seeded by G(N-1,M-1) = w, and
+//   dL/dq(i,j) = G(i,j) ((K[i,j+1] + K[i+1,j]) (1/2 + q/6) + K[i,j] q/6).
+// Rows are swept bottom-up and columns right to left in increment form:
+// with H(i,j) = G(i,j) - G(i+1,j),
+//   H(i,j) = H(i,j+1) + (A(i+1,j)-1) G(i+1,j) + (A(i,j+1)-1) G(i,j+1)
+//            + (1-B(i+1,j+1)) G(i+1,j+1),
+// which keeps FP32 rounding small, as the forward's increment form does.
+// The seed enters as H(N-1, M) = w.
 //
-// Phase 1 (per pair): reversed sweep; G is stored to per-warp scratch.
-// Phase 2: forward sweep over the original grid; each refined cell reads
-// Lam[i+1,j+1] = G(N-1-i, M-1-j) and adds dL/dZ of its cell.  Zbar is
-// pulled back through the second difference -- each lane takes the part of
-// Mbar that comes from its own cells, and the parts of neighbouring lanes
-// add up to the full Mbar -- and through the static kernel into dX (one
-// grid row per lane per step, atomics) and dparam.
+// One warp per pair; lane l owns C cell columns (C*F refined columns) of a
+// strip of 32*C-1 cells, as in the forward sweep.
+// Phase 1 is the forward sweep (lane l one row behind lane l-1).  Every lane
+// records the K values of its refined rows, and of the column to its left,
+// per step in a lane-minor layout [step][f][column][lane], so the stores of
+// a warp are contiguous.
+// Phase 2 is its exact time reversal: lane l is one row behind lane l+1, so
+// the adjoint's row increments H, the G values at the lane boundary and the
+// neighbouring cell's q arrive from lane l+1 by __shfl_down.  Every lane
+// reads the record slot of the same step: the loads are contiguous too.
+// It forms dL/dZ per cell and pulls it back through the second difference
+// and the static kernel into dX and dparam like the DP adjoint: lane l
+// covers its C grid columns plus the next lane's first one, and the dX
+// vector of a grid row is summed along the lanes and added once per row
+// and strip.
 #pragma once
 
 #include "common.cuh"
@@ -50,47 +55,53 @@ struct PdeBwdArgs {
   T* dX;                  // [nX, LX, d] row-side gradient (accumulated)
   int LX, d;
   double* dparam;         // may be null
-  T* scratch;             // per warp: G grid, then the strip boundary buffer
+  T* scratch;             // per warp, see pde_bwd_scratch_elems
   long long scratch_per_warp;
-  long long grid_stride;  // row stride of G (>= refined columns)
-  long long bb_off;       // offset of the boundary buffer in a warp's scratch
-  int rows_max;           // cell rows the boundary buffer holds
+  int ns_max, rows_max;
   int* status;
 };
 
-// W-wide vector of T (W * sizeof(T) <= 16) for the adjoint-grid traffic.
-template <typename T, int W> struct VecW;
-template <> struct VecW<float, 1> { using type = float; };
-template <> struct VecW<float, 2> { using type = float2; };
-template <> struct VecW<float, 4> { using type = float4; };
-template <> struct VecW<double, 1> { using type = double; };
-template <> struct VecW<double, 2> { using type = double2; };
+// Scratch elements per warp:
+//   REC [ns_max][rows_max + 32][F][C*F + 1][32]  K records of phase 1
+//   BL  [2][rows_max][2F]                         forward strip carries
+//   BR  [2][rows_max][2F + 1]                     adjoint strip carries
+__host__ __device__ inline long long pde_bwd_scratch_elems(int ns_max, int rows_max, int c,
+                                                           int f) {
+  return (long long)ns_max * (rows_max + 32) * f * (c * f + 1) * 32 +
+         2LL * rows_max * 2 * f + 2LL * rows_max * (2 * f + 1);
+}
 
 template <typename T, int KD, int C, int F, int WPB>
 __global__ void __launch_bounds__(WPB * 32)
 pde_bwd_kernel(const PdeBwdArgs<T> args) {
-  // A lane's F refined columns of one cell are contiguous in G (reversed in
-  // phase 2), so they move as W-wide vectors: the grid row base and the
-  // per-warp scratch are 16-byte aligned and F * (cell column) is a
-  // multiple of W.
-  constexpr int GW0 = 16 / (int)sizeof(T);
-  constexpr int GW = F < GW0 ? F : GW0;
-  using GV = typename VecW<T, GW>::type;
   constexpr int RS = packed_stride<T>(KD);
   constexpr int VN = Vec<T>::N;
   using V = typename Vec<T>::type;
   constexpr int STRIP = 32 * C - 1;
-  constexpr int NXE = 2 * F + 2;  // per cell row: K, H per refined row, Z, Z(row above)
+  constexpr int CF = C * F;
+  constexpr int RW = CF + 1;     // record row: CF refined columns + the left column
+  constexpr int NB = 2 * F + 1;  // adjoint carry: H and G per refined row, q of the cell
   constexpr T invF2 = T(1) / T(F * F);
 
   const int lane = threadIdx.x & 31;
   const long long wg = (long long)blockIdx.x * WPB + (threadIdx.x >> 5);
   const long long nw = (long long)gridDim.x * WPB;
-  T* Gs = args.scratch + wg * args.scratch_per_warp;
-  T* BB = Gs + args.bb_off;
-  const long long GS = args.grid_stride;
+  T* scr = args.scratch + wg * args.scratch_per_warp;
+  const long long steps = (long long)args.rows_max + 32;
+  const long long rm = args.rows_max;
+  T* REC = scr;
+  T* BL = REC + (long long)args.ns_max * steps * F * RW * 32;
+  T* BR = BL + 2 * rm * 2 * F;
+  auto rec_at = [&](int s, long long t) {
+    return REC + ((long long)s * steps + t) * F * RW * 32 + lane;
+  };
+
   const double alpha = 1.4426950408889634 / fmax(2.0 * args.param * args.param, 1e-12);
   const bool rbf = args.kind == KIND_RBF;
+  const bool want_dpar = args.dparam != nullptr;
+  const T inv2a = T(1.0 / (2.0 * alpha));
+  const double xscale = rbf ? 1.0 / (args.param * args.param) : args.param;
+  double dpar_w = 0.0;
 
   for (long long tid = wg; tid < args.ntasks; tid += nw) {
     const int2 ab = decode_task((int)tid, args.mode, args.nY, args.list, args.order);
@@ -104,23 +115,21 @@ pde_bwd_kernel(const PdeBwdArgs<T> args) {
     const int lx = Lx - 1, ly = Ly - 1;
     if (lx <= 0 || ly <= 0) continue;  // K = 1: no gradient
     const int ns = (ly + STRIP - 1) / STRIP;
-    if (ns > 1 && lx > args.rows_max) {
+    if (ns > args.ns_max || lx > args.rows_max) {
       if (lane == 0) set_status(args.status, KSIG_ERR_DEVICE);
       continue;
     }
-    const int N = lx * F, M = ly * F;
     const T w = (T)args.grad[task];
     const T* xb = args.xr + args.xstart[a] * RS;
     const T* yb = args.yr + args.ystart[b] * RS;
 
-    // The lane's C+1 grid columns of strip s (phase 1: reversed grid).
+    // The lane's C+1 grid columns of strip s.
     T yv[C + 1][KD + 1];
-    auto load_y = [&](int s, bool rev) {
+    auto load_y = [&](int s) {
 #pragma unroll
       for (int c = 0; c <= C; ++c) {
         int col = s * STRIP + C * lane + c;
         col = col < Ly - 1 ? col : Ly - 1;
-        if (rev) col = Ly - 1 - col;
         const V* p = reinterpret_cast<const V*>(yb + (long long)col * RS);
         T tmp[RS];
 #pragma unroll
@@ -129,10 +138,10 @@ pde_bwd_kernel(const PdeBwdArgs<T> args) {
         for (int k = 0; k <= KD; ++k) yv[c][k] = tmp[k];
       }
     };
-    auto gram = [&](int row, bool rev, T (&m)[C + 1], T (&arg)[C + 1], T (&xv)[RS]) {
-      row = row < Lx - 1 ? row : Lx - 1;
-      if (rev) row = Lx - 1 - row;
+    auto gram = [&](int row, T (&m)[C + 1], T (&arg)[C + 1]) {
+      row = row < 0 ? 0 : (row > lx ? lx : row);
       const V* p = reinterpret_cast<const V*>(xb + (long long)row * RS);
+      T xv[RS];
 #pragma unroll
       for (int v = 0; v < RS / VN; ++v) reinterpret_cast<V*>(xv)[v] = __ldg(p + v);
 #pragma unroll
@@ -145,52 +154,47 @@ pde_bwd_kernel(const PdeBwdArgs<T> args) {
       }
     };
 
-    // ------------------------- phase 1: reversed adjoint sweep -------------
+    // ------------- phase 1: forward, top-down, strips left to right --------
     for (int s = 0; s < ns; ++s) {
-      load_y(s, true);
+      load_y(s);
       const int g0 = s * STRIP + C * lane;
-      T Mlo[C + 1], Mhi[C + 1], argd[C + 1], xv[RS];
-      gram(0, true, Mlo, argd, xv);
-      T Kr[C * F];
+      const T* blin = BL + (long long)((s + 1) & 1) * rm * 2 * F;  // from strip s - 1
+      T* blout = BL + (long long)(s & 1) * rm * 2 * F;
+      T Mlo[C + 1], Mhi[C + 1], argd[C + 1];
+      gram(0, Mlo, argd);
+      T Kr[CF];
 #pragma unroll
-      for (int j = 0; j < C * F; ++j) Kr[j] = T(0);
-      T kcorner = T(0);
-      T X[NXE];
+      for (int j = 0; j < CF; ++j) Kr[j] = T(1);
+      T kcorner = T(1);
+      T X[2 * F];  // outgoing: K of the last refined column, H, per refined row
 #pragma unroll
-      for (int h = 0; h < NXE; ++h) X[h] = T(0);
-      T Zprev[C];
-#pragma unroll
-      for (int c = 0; c < C; ++c) Zprev[c] = T(0);
+      for (int h = 0; h < 2 * F; ++h) X[h] = T(0);
       for (int t = 0; t < lx + 32; ++t) {
-        const int r = t - lane;  // reversed cell row of this lane
-        T Xin[NXE];
+        const int r = t - lane;
+        T Xin[2 * F];
 #pragma unroll
-        for (int h = 0; h < NXE; ++h) Xin[h] = shfl_up(X[h], 1);
+        for (int h = 0; h < 2 * F; ++h) Xin[h] = shfl_up(X[h], 1);
         if (r >= 0 && r < lx) {
-          gram(r + 1, true, Mhi, argd, xv);
-          T Z[C];
+          gram(r + 1, Mhi, argd);
+          if (lane == 0) {
+            if (s > 0) {
+#pragma unroll
+              for (int h = 0; h < 2 * F; ++h) Xin[h] = __ldcg(blin + (long long)r * 2 * F + h);
+            } else {
+#pragma unroll
+              for (int f = 0; f < F; ++f) { Xin[f] = T(1); Xin[F + f] = T(0); }
+            }
+          }
+          T a_[C], b_[C];
 #pragma unroll
           for (int c = 0; c < C; ++c) {
             const bool valid = g0 + c < ly && !(lane == 31 && c == C - 1);
-            Z[c] = valid ? (Mhi[c + 1] - Mhi[c] - Mlo[c + 1] + Mlo[c]) : T(0);
+            const T z = valid ? (Mhi[c + 1] - Mhi[c] - Mlo[c + 1] + Mlo[c]) : T(0);
+            const T q = z * invF2;
+            b_[c] = q * q * (T(1) / T(12));
+            a_[c] = fma(T(0.5), q, b_[c]);
           }
-          if (lane == 0) {
-            if (s > 0) {
-              const T* src = BB + (long long)r * NXE;
-#pragma unroll
-              for (int h = 0; h < NXE; ++h) Xin[h] = __ldcg(src + h);
-            } else {
-#pragma unroll
-              for (int h = 0; h < NXE; ++h) Xin[h] = T(0);
-              if (r == 0) Xin[F] = w;  // seed G(0,0) = w through the left H
-            }
-          }
-          // Z of the cell columns left-extended by the left neighbour's cell.
-          T Zx[C + 1], Zpx[C + 1];
-          Zx[0] = Xin[2 * F];
-          Zpx[0] = Xin[2 * F + 1];
-#pragma unroll
-          for (int c = 0; c < C; ++c) { Zx[c + 1] = Z[c]; Zpx[c + 1] = Zprev[c]; }
+          T* rp = rec_at(s, t);
 #pragma unroll
           for (int f = 0; f < F; ++f) {
             T klo = (f == 0) ? kcorner : Xin[f > 0 ? f - 1 : 0];
@@ -201,18 +205,9 @@ pde_bwd_kernel(const PdeBwdArgs<T> args) {
               const bool skip = (c == C - 1) && lane == 31;
 #pragma unroll
               for (int g = 0; g < F; ++g) {
-                // Refined point (rF+f, (g0+c)F+g); its own cell is the refined
-                // cell up-left of it, Ar the cell above, Ab the cell to the left.
-                const T z_up = (f > 0) ? Zx[c + 1] : Zpx[c + 1];
-                const T z_left = (g > 0) ? Zx[c + 1] : Zx[c];
-                const T z_ul = (f > 0) ? z_left : ((g > 0) ? Zpx[c + 1] : Zpx[c]);
-                const T qr = z_up * invF2, qb = z_left * invF2, qo = z_ul * invF2;
-                const T ar = qr * fma(qr, T(1) / T(12), T(0.5));
-                const T ab_ = qb * fma(qb, T(1) / T(12), T(0.5));
-                const T bq = qo * qo * (T(1) / T(12));
                 const int J = c * F + g;
                 const T kro = Kr[J];
-                const T gg = fma(ar, kro, fma(ab_, kln, bq * klo));
+                const T gg = fma(kro + kln, a_[c], klo * b_[c]);
                 const T Hn = H + gg;
                 const T krn = kro + Hn;
                 if (!skip) {
@@ -225,207 +220,212 @@ pde_bwd_kernel(const PdeBwdArgs<T> args) {
             }
             X[f] = kln;
             X[F + f] = H;
-            // Store G at refined row rF+f for the lane's refined columns.
-            const long long grow = (long long)r * F + f;
+            // Record refined row f: K at its lower corners, and at the
+            // column left of the lane.
 #pragma unroll
-            for (int c = 0; c < C; ++c) {
-              const bool valid = g0 + c < ly && !(lane == 31 && c == C - 1);
-              if (valid) {
-                GV* dst = reinterpret_cast<GV*>(Gs + grow * GS + (long long)(g0 + c) * F);
-#pragma unroll
-                for (int v = 0; v < F / GW; ++v) {
-                  GV gv;
-                  T* e = reinterpret_cast<T*>(&gv);
-#pragma unroll
-                  for (int i = 0; i < GW; ++i) e[i] = Kr[c * F + v * GW + i];
-                  __stcg(dst + v, gv);
-                }
-              }
-            }
+            for (int j = 0; j < CF; ++j) rp[(f * RW + j) * 32] = Kr[j];
+            rp[(f * RW + CF) * 32] = Xin[f];
           }
           kcorner = Xin[F - 1];
-          // Z of this lane's last valid cell (this row, row above) for the
-          // lane to the right.
-          X[2 * F] = (lane == 31) ? Z[C >= 2 ? C - 2 : 0] : Z[C - 1];
-          X[2 * F + 1] = (lane == 31) ? Zprev[C >= 2 ? C - 2 : 0] : Zprev[C - 1];
           if (lane == 31 && s + 1 < ns) {
-            T* dst = BB + (long long)r * NXE;
 #pragma unroll
-            for (int h = 0; h < NXE; ++h) __stcg(dst + h, X[h]);
+            for (int h = 0; h < 2 * F; ++h) __stcg(blout + (long long)r * 2 * F + h, X[h]);
           }
-#pragma unroll
-          for (int c = 0; c < C; ++c) Zprev[c] = Z[c];
 #pragma unroll
           for (int c = 0; c <= C; ++c) Mlo[c] = Mhi[c];
         }
-        __syncwarp();
       }
+      __syncwarp();  // carries and records of this strip -> later readers
     }
-    __syncwarp();
 
-    // ------------------------- phase 2: forward + gradient ----------------
-    double dpar = 0.0;
-    const double scale_x = rbf ? 1.0 / (args.param * args.param) : args.param;
-    for (int s = 0; s < ns; ++s) {
-      load_y(s, false);
+    // ------------- phase 2: adjoint, bottom-up, strips right to left -------
+    for (int s = ns - 1; s >= 0; --s) {
+      load_y(s);
       const int g0 = s * STRIP + C * lane;
-      T Mlo[C + 1], arglo[C + 1], Mhi[C + 1], arghi[C + 1], xlo[RS], xhi[RS];
-      gram(0, false, Mlo, arglo, xlo);
-      T Kr[C * F];
+      const T* brin = BR + (long long)((s + 1) & 1) * rm * NB;  // from strip s + 1
+      T* brout = BR + (long long)(s & 1) * rm * NB;
+      T Mprev[C + 1], argprev[C + 1];
 #pragma unroll
-      for (int j = 0; j < C * F; ++j) Kr[j] = T(1);
-      T kcorner = T(1);
-      T X[NXE];
+      for (int c = 0; c <= C; ++c) { Mprev[c] = T(0); argprev[c] = T(0); }
+      T Zprev[C], Zbprev[C];
 #pragma unroll
-      for (int h = 0; h < NXE; ++h) X[h] = T(0);
-      T Zbp[C];  // Zbar of the row above (this lane's cells)
+      for (int c = 0; c < C; ++c) { Zprev[c] = T(0); Zbprev[c] = T(0); }
+      T Gb[CF];  // G of the refined row below the current cell row
 #pragma unroll
-      for (int c = 0; c < C; ++c) Zbp[c] = T(0);
-      for (int t = 0; t < lx + 1 + 32; ++t) {
-        const int r = t - lane;  // cell row of this lane; r == lx finishes grid row lx
-        T Xin[NXE];
+      for (int j = 0; j < CF; ++j) Gb[j] = T(0);
+      T Aprev[NB];
 #pragma unroll
-        for (int h = 0; h < NXE; ++h) Xin[h] = shfl_up(X[h], 1);
-        if (r >= 0 && r <= lx) {
-          T Zb[C];
+      for (int h = 0; h < NB; ++h) Aprev[h] = T(0);
+      T accprev[KD + 1];
 #pragma unroll
-          for (int c = 0; c < C; ++c) Zb[c] = T(0);
-          if (r < lx) {
-            gram(r + 1, false, Mhi, arghi, xhi);
-            T Z[C];
+      for (int k = 0; k <= KD; ++k) accprev[k] = T(0);
+      T gr_below = T(0), zr_below = T(0);  // lane l+1's G and q one cell row down
+      for (int u = 0; u < lx + 33; ++u) {
+        const int rho = u - (31 - lane);
+        const int r = lx - rho;                      // cell row; grid row computed
+        const bool act = rho >= 1 && rho <= lx;      // cell row r exists
+        const bool fin = rho >= 1 && rho <= lx + 1;  // grid row r + 1 completes here
+        T Ain[NB];
 #pragma unroll
-            for (int c = 0; c < C; ++c) Z[c] = Mhi[c + 1] - Mhi[c] - Mlo[c + 1] + Mlo[c];
-            if (lane == 0) {
-              if (s > 0) {
-                const T* src = BB + (long long)r * NXE;
+        for (int h = 0; h < NB; ++h) Ain[h] = shfl_down(Aprev[h], 1);
+        T acc[KD + 1];
 #pragma unroll
-                for (int h = 0; h < 2 * F; ++h) Xin[h] = __ldcg(src + h);
-              } else {
+        for (int k = 0; k <= KD; ++k) acc[k] = shfl_down(accprev[k], 1);
+        if (lane == 31) {
 #pragma unroll
-                for (int f = 0; f < F; ++f) { Xin[f] = T(1); Xin[F + f] = T(0); }
+          for (int k = 0; k <= KD; ++k) acc[k] = T(0);
+#pragma unroll
+          for (int h = 0; h < NB; ++h)
+            Ain[h] = (s + 1 < ns && act) ? __ldcg(brin + (long long)r * NB + h) : T(0);
+          if (s + 1 == ns && act && r == lx - 1) Ain[F - 1] = w;  // seed H(N-1, M) = w
+        }
+        T Mnew[C + 1], argn[C + 1];
+        gram(r, Mnew, argn);
+        T Z[C], Zb[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+          const bool valid = act && g0 + c < ly && !(lane == 31 && c == C - 1);
+          Z[c] = valid ? (Mprev[c + 1] - Mprev[c] - Mnew[c + 1] + Mnew[c]) : T(0);
+          Zb[c] = T(0);
+        }
+        T Aout[NB];
+#pragma unroll
+        for (int h = 0; h < NB; ++h) Aout[h] = T(0);
+        if (act) {
+          const long long t = (long long)lx + 31 - u;  // phase-1 step of this cell row
+          const T* rb = rec_at(s, t);
+          const T* ra = rec_at(s, t - 1);               // the cell row above (r > 0)
+          T Kbot[RW], Ktop[RW];
+#pragma unroll
+          for (int j = 0; j < RW; ++j) Kbot[j] = rb[((F - 1) * RW + j) * 32];
+          T Gbel[CF], Gcur[CF];
+#pragma unroll
+          for (int j = 0; j < CF; ++j) { Gbel[j] = Gb[j]; Gcur[j] = T(0); }
+#pragma unroll
+          for (int f = F - 1; f >= 0; --f) {
+            if (f > 0) {
+#pragma unroll
+              for (int j = 0; j < RW; ++j) Ktop[j] = rb[((f > 0 ? f - 1 : 0) * RW + j) * 32];
+            } else if (r > 0) {
+#pragma unroll
+              for (int j = 0; j < RW; ++j) Ktop[j] = ra[((F - 1) * RW + j) * 32];
+            } else {
+#pragma unroll
+              for (int j = 0; j < RW; ++j) Ktop[j] = T(1);
+            }
+            const bool last_f = f == F - 1;
+            T H = Ain[f];
+            T Gr = Ain[F + f];
+            T Gbr = last_f ? gr_below : Ain[F + (f + 1 < F ? f + 1 : 0)];
+            T qr_cell = Ain[2 * F] * invF2;
+            T qo_cell = last_f ? zr_below * invF2 : qr_cell;
+#pragma unroll
+            for (int c = C - 1; c >= 0; --c) {
+              const bool skip = (c == C - 1) && lane == 31;
+              const T qown = Z[c] * invF2;
+              const T qb = last_f ? Zprev[c] * invF2 : qown;
+              const T abq = qb * fma(qb, T(1) / T(12), T(0.5));
+              const T q6 = qown * (T(1) / T(6));
+              T zb = T(0);
+#pragma unroll
+              for (int g = F - 1; g >= 0; --g) {
+                const int J = c * F + g;
+                const T qr = (g < F - 1) ? qown : qr_cell;
+                const T qo = (g < F - 1) ? qb : qo_cell;
+                const T arq = qr * fma(qr, T(1) / T(12), T(0.5));
+                const T boq = qo * qo * (T(1) / T(12));
+                const T Gbelow = Gbel[J];
+                const T Hn = fma(abq, Gbelow, fma(arq, Gr, fma(boq, Gbr, H)));
+                const T G = Gbelow + Hn;
+                const T Ktr = Ktop[J];
+                const T Ktl = J > 0 ? Ktop[J > 0 ? J - 1 : 0] : Ktop[CF];
+                const T Kbl = J > 0 ? Kbot[J > 0 ? J - 1 : 0] : Kbot[CF];
+                const T dq = G * fma(Ktr + Kbl, T(0.5) + q6, Ktl * q6);
+                if (!skip) {
+                  H = Hn;
+                  Gr = G;
+                  Gbr = Gbelow;
+                  Gcur[J] = G;
+                  zb += dq;
+                }
+              }
+              Zb[c] += zb;
+              if (!skip) {
+                qr_cell = qown;
+                qo_cell = qb;
               }
             }
-            T a_[C], b_[C], qv[C];
+            Aout[f] = H;
+            Aout[F + f] = Gr;
 #pragma unroll
-            for (int c = 0; c < C; ++c) {
-              const T q = Z[c] * invF2;
-              qv[c] = q;
-              b_[c] = q * q * (T(1) / T(12));
-              a_[c] = fma(T(0.5), q, b_[c]);
-            }
+            for (int j = 0; j < CF; ++j) Gbel[j] = Gcur[j];
 #pragma unroll
-            for (int f = 0; f < F; ++f) {
-              T klo = (f == 0) ? kcorner : Xin[f > 0 ? f - 1 : 0];
-              T kln = Xin[f];
-              T H = Xin[F + f];
-              // Lam[i+1, j+1] = G(N-1-i, M-1-j) for refined row i = rF+f.
-              const long long grow = (long long)(N - 1 - (r * F + f));
-#pragma unroll
-              for (int c = 0; c < C; ++c) {
-                const bool skip = (c == C - 1) && lane == 31;
-                const bool valid = g0 + c < ly && !skip;
-                // Lam of the cell's F refined columns: G columns
-                // M - (g0+c+1)F .. M - (g0+c)F - 1, in reverse.
-                T lamv[F];
-                if (valid) {
-                  const GV* src = reinterpret_cast<const GV*>(
-                      Gs + grow * GS + (long long)(M - (g0 + c + 1) * F));
-#pragma unroll
-                  for (int v = 0; v < F / GW; ++v) {
-                    const GV gv = __ldcg(src + v);
-                    const T* e = reinterpret_cast<const T*>(&gv);
-#pragma unroll
-                    for (int i = 0; i < GW; ++i) lamv[F - 1 - (v * GW + i)] = e[i];
-                  }
-                } else {
-#pragma unroll
-                  for (int g = 0; g < F; ++g) lamv[g] = T(0);
-                }
-#pragma unroll
-                for (int g = 0; g < F; ++g) {
-                  const int J = c * F + g;
-                  const T kro = Kr[J];
-                  const T gg = fma(kro + kln, a_[c], klo * b_[c]);
-                  const T Hn = H + gg;
-                  const T krn = kro + Hn;
-                  if (valid) {
-                    const T lam = lamv[g];
-                    const T q6 = qv[c] * (T(1) / T(6));
-                    Zb[c] = fma(lam, fma(kro + kln, T(0.5) + q6, klo * q6), Zb[c]);
-                  }
-                  if (!skip) {
-                    klo = kro;
-                    kln = krn;
-                    H = Hn;
-                    Kr[J] = krn;
-                  }
-                }
-              }
-              X[f] = kln;
-              X[F + f] = H;
-            }
-            kcorner = Xin[F - 1];
-            if (lane == 31 && s + 1 < ns) {
-              T* dst = BB + (long long)r * NXE;
-#pragma unroll
-              for (int h = 0; h < 2 * F; ++h) __stcg(dst + h, X[h]);
-            }
-#pragma unroll
-            for (int c = 0; c < C; ++c) {
-              const bool valid = g0 + c < ly && !((c == C - 1) && lane == 31);
-              Zb[c] = valid ? Zb[c] * invF2 : T(0);
-            }
+            for (int j = 0; j < RW; ++j) Kbot[j] = Ktop[j];
           }
-          // Grid row r: Mbar from this lane's cells of rows r-1 (Zbp) and r
-          // (Zb), on the lane's grid columns g0 .. g0+C.
-          T q[KD];
+          Aout[2 * F] = Z[0];
 #pragma unroll
-          for (int k = 0; k < KD; ++k) q[k] = T(0);
-          T sw = T(0);
-          const T inv2a = T(1) / T(2.0 * alpha);
+          for (int j = 0; j < CF; ++j) Gb[j] = Gbel[j];
 #pragma unroll
-          for (int c = 0; c <= C; ++c) {
-            const T lo_l = (c > 0) ? Zb[c > 0 ? c - 1 : 0] : T(0);
-            const T lo_r = (c < C) ? Zb[c < C ? c : 0] : T(0);
-            const T hi_l = (c > 0) ? Zbp[c > 0 ? c - 1 : 0] : T(0);
-            const T hi_r = (c < C) ? Zbp[c < C ? c : 0] : T(0);
-            // Mbar(r, j) = Zbar(r-1, j-1) - Zbar(r-1, j) - Zbar(r, j-1) + Zbar(r, j)
-            const T mbar = hi_l - hi_r - lo_l + lo_r;
-            const bool col_ok = g0 + c < Ly;
-            const T W = col_ok ? (rbf ? mbar * Mlo[c] : mbar) : T(0);
-            sw += W;
-#pragma unroll
-            for (int k = 0; k < KD; ++k) q[k] = fma(W, yv[c][k], q[k]);
-            if (col_ok)
-              dpar += rbf ? (double)W * (-(double)arglo[c] / alpha) : (double)W * (double)Mlo[c];
+          for (int c = 0; c < C; ++c) {
+            const bool valid = g0 + c < ly && !(lane == 31 && c == C - 1);
+            Zb[c] = valid ? Zb[c] * invF2 : T(0);
           }
-          if (rbf) {
+          if (lane == 0 && s > 0) {
 #pragma unroll
-            for (int k = 0; k < KD; ++k) q[k] -= sw * (xlo[k] * inv2a);
-          }
-          T* dst = args.dX + ((long long)a * args.LX + r) * args.d;
-#pragma unroll
-          for (int k = 0; k < KD; ++k)
-            if (k < args.d && q[k] != T(0)) atomicAdd(dst + k, (T)(scale_x * (double)q[k]));
-#pragma unroll
-          for (int c = 0; c < C; ++c) Zbp[c] = Zb[c];
-          if (r < lx) {
-#pragma unroll
-            for (int c = 0; c <= C; ++c) { Mlo[c] = Mhi[c]; arglo[c] = arghi[c]; }
-#pragma unroll
-            for (int k = 0; k < RS; ++k) xlo[k] = xhi[k];
+            for (int h = 0; h < NB; ++h) __stcg(brout + (long long)r * NB + h, Aout[h]);
           }
         }
-        __syncwarp();
-      }
-    }
-    if (args.dparam) {
+
+        // ---- grid row p = r + 1: partial Mbar of this lane's cells ----
+        const int p = r + 1;
+        T dp = T(0);
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) dpar += __shfl_xor_sync(FULL, dpar, o);
-      if (lane == 0) {
-        const double p = args.param;
-        atomicAdd(args.dparam, rbf ? dpar / (p * p * p) : dpar / p);
+        for (int c = 0; c <= C; ++c) {
+          T mb = (c < C) ? Zbprev[c < C ? c : 0] - Zb[c < C ? c : 0] : T(0);
+          if (c > 0) mb += Zb[c - 1] - Zbprev[c - 1];
+          const int q = g0 + c;
+          const bool valid = fin && q < Ly && (c < C || lane < 31);
+          const T W = valid ? (rbf ? mb * Mprev[c] : mb) : T(0);
+#pragma unroll
+          for (int k = 0; k < KD; ++k) acc[k] = fma(W, yv[c][k], acc[k]);
+          acc[KD] += W;
+          dp = fma(W, rbf ? argprev[c] : Mprev[c], dp);
+        }
+        if (want_dpar) dpar_w += (double)dp;
+        if (lane == 0 && fin) {
+          const V* xp = reinterpret_cast<const V*>(xb + (long long)p * RS);
+          T xv[RS];
+#pragma unroll
+          for (int v = 0; v < RS / VN; ++v) reinterpret_cast<V*>(xv)[v] = __ldg(xp + v);
+          T* dst = args.dX + ((long long)a * args.LX + p) * args.d;
+#pragma unroll
+          for (int k = 0; k < KD; ++k) {
+            if (k < args.d) {
+              const T v = rbf ? acc[k] - acc[KD] * (xv[k] * inv2a) : acc[k];
+              atomicAdd(dst + k, (T)(xscale * (double)v));
+            }
+          }
+        }
+#pragma unroll
+        for (int k = 0; k <= KD; ++k) accprev[k] = acc[k];
+        gr_below = Ain[F];
+        zr_below = Ain[2 * F];
+#pragma unroll
+        for (int h = 0; h < NB; ++h) Aprev[h] = Aout[h];
+#pragma unroll
+        for (int c = 0; c < C; ++c) { Zprev[c] = Z[c]; Zbprev[c] = Zb[c]; }
+#pragma unroll
+        for (int c = 0; c <= C; ++c) { Mprev[c] = Mnew[c]; argprev[c] = argn[c]; }
       }
+      __syncwarp();  // adjoint carries of this strip -> the next strip
+    }
+  }
+  if (want_dpar) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dpar_w += __shfl_xor_sync(FULL, dpar_w, o);
+    if (lane == 0 && dpar_w != 0.0) {
+      const double p = args.param;
+      atomicAdd(args.dparam, rbf ? -dpar_w / (alpha * p * p * p) : dpar_w / p);
     }
   }
 }

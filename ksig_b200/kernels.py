@@ -189,7 +189,9 @@ class SignatureBase:
       return K
     if K.requires_grad:
       return K
-    return K.detach().cpu().numpy()
+    out = K.detach().cpu().numpy()
+    E.check_device_status()  # the copy above has synchronised already
+    return out
 
   def _param_tensor(self):
     sk = self.static_kernel

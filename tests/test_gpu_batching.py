@@ -119,3 +119,21 @@ def test_autotune_picks_a_width_and_keeps_results():
   finally:
     tuning.reset()
   assert tuning.get_cols(tuning.OP_DP_FWD) == 0
+
+
+def test_device_status_reaches_python():
+  """A length beyond the padded extent is clamped on the device and flagged
+  in the workspace status word; the Python layer raises it at the next
+  check instead of returning silently."""
+  import ksig_b200 as K
+  from ksig_b200 import _engine as E, _lib as Lb
+  K.check_device_status()  # clean slate
+  X = torch.randn((3, 10, 2), device='cuda')
+  bad = E.Seqs(X, torch.tensor([10, 12, 5], dtype=torch.int32, device='cuda'))
+  E.sig_levels(bad, None, Lb.PAIRS_UPPER, 3, 1, True, Lb.STATIC_RBF, 1.0)
+  with pytest.raises(ValueError):
+    K.check_device_status()
+  K.check_device_status()  # cleared by the raise
+  good = E.Seqs(X, torch.tensor([10, 7, 5], dtype=torch.int32, device='cuda'))
+  E.sig_levels(good, None, Lb.PAIRS_UPPER, 3, 1, True, Lb.STATIC_RBF, 1.0)
+  K.check_device_status()
