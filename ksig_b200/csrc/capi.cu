@@ -573,6 +573,7 @@ struct PdeBwdPlan {
   FwdPlan f;
   const KernelEntry* k;
   int c, F, grid, rows_max, ns_max;
+  size_t dyn_smem;
   long long scratch_per_warp;
   size_t off_scratch, total;
 };
@@ -613,12 +614,15 @@ int plan_pde_bwd(int nX, int LX, int nY, int LY, int d, int dtype, int dyadic, i
   bp.ns_max = ly <= strip ? 1 : (ly + strip - 1) / strip;
   bp.scratch_per_warp = (pde_bwd_scratch_elems(bp.ns_max, bp.rows_max, bp.c, bp.F) + 3) / 4 * 4;
   const size_t es = bp.f.f64 ? 8 : 4;
+  bp.dyn_smem = pde_bwd_smem_bytes(k->wpb, bp.c, bp.F, es);
+  cudaError_t e = ensure_smem_attr(k->func, bp.dyn_smem);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(pde backward)");
   int occ = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k->func, k->wpb * 32, 0);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k->func, k->wpb * 32, bp.dyn_smem);
   if (e != cudaSuccess || occ <= 0) occ = 1;
   const int sms = sm_count() > 0 ? sm_count() : 148;
   long long warps = (long long)sms * occ * k->wpb;
-  // The K records grow with rows x strips; keep the scratch within a budget.
+  // The records grow with rows x strips; keep the scratch within a budget.
   const long long budget = (long long)env_int("KSIG_PDE_BWD_SCRATCH_MB", 16384) << 20;
   const long long cap = budget / (long long)(bp.scratch_per_warp * es);
   if (warps > cap) warps = cap > (long long)k->wpb ? cap : k->wpb;
@@ -674,7 +678,7 @@ int run_pde_bwd(const PdeBwdPlan& bp, const void* X, const int32_t* lenX, int nX
   a.rows_max = bp.rows_max;
   a.status = status;
   void* kargs[] = {&a};
-  KSIG_CUDA(launch_main(bp.k->func, dim3(bp.grid), dim3(bp.k->wpb * 32), kargs, 0, st));
+  KSIG_CUDA(launch_main(bp.k->func, dim3(bp.grid), dim3(bp.k->wpb * 32), kargs, bp.dyn_smem, st));
   return KSIG_OK;
 }
 

@@ -18,14 +18,18 @@
 //
 // One warp per pair; lane l owns C cell columns (C*F refined columns) of a
 // strip of 32*C-1 cells, as in the forward sweep.
-// Phase 1 is the forward sweep (lane l one row behind lane l-1).  Every lane
-// records the K values of its refined rows, and of the column to its left,
-// per step in a lane-minor layout [step][f][column][lane], so the stores of
-// a warp are contiguous.
+// Phase 1 is the forward sweep (lane l one row behind lane l-1).  Per step
+// every lane records only the boundary of its block of the K grid: the
+// bottom refined row (C*F values) and the K and H values it received from
+// the left (2F values), in a lane-minor layout [step][value][lane], so the
+// stores of a warp are contiguous.
 // Phase 2 is its exact time reversal: lane l is one row behind lane l+1, so
 // the adjoint's row increments H, the G values at the lane boundary and the
 // neighbouring cell's q arrive from lane l+1 by __shfl_down.  Every lane
-// reads the record slot of the same step: the loads are contiguous too.
+// reads the record slots of the same step (contiguous loads), rebuilds the
+// F x C*F interior of its K block with the forward's own arithmetic (so the
+// values are the forward's, bit for bit) into shared memory, and runs the
+// adjoint over it.
 // It forms dL/dZ per cell and pulls it back through the second difference
 // and the static kernel into dX and dparam like the DP adjoint: lane l
 // covers its C grid columns plus the next lane's first one, and the dX
@@ -62,13 +66,19 @@ struct PdeBwdArgs {
 };
 
 // Scratch elements per warp:
-//   REC [ns_max][rows_max + 32][F][C*F + 1][32]  K records of phase 1
-//   BL  [2][rows_max][2F]                         forward strip carries
-//   BR  [2][rows_max][2F + 1]                     adjoint strip carries
+//   REC [ns_max][rows_max + 32][C*F + 2F][32]  boundary records of phase 1
+//   BL  [2][rows_max][2F]                       forward strip carries
+//   BR  [2][rows_max][2F + 1]                   adjoint strip carries
 __host__ __device__ inline long long pde_bwd_scratch_elems(int ns_max, int rows_max, int c,
                                                            int f) {
-  return (long long)ns_max * (rows_max + 32) * f * (c * f + 1) * 32 +
+  return (long long)ns_max * (rows_max + 32) * (c * f + 2 * f) * 32 +
          2LL * rows_max * 2 * f + 2LL * rows_max * (2 * f + 1);
+}
+
+// Dynamic shared memory per block: the rebuilt K block of each lane,
+// [F][C*F + 1][32] per warp.
+__host__ __device__ inline size_t pde_bwd_smem_bytes(int wpb, int c, int f, size_t es) {
+  return (size_t)wpb * f * (c * f + 1) * 32 * es;
 }
 
 template <typename T, int KD, int C, int F, int WPB>
@@ -79,21 +89,24 @@ pde_bwd_kernel(const PdeBwdArgs<T> args) {
   using V = typename Vec<T>::type;
   constexpr int STRIP = 32 * C - 1;
   constexpr int CF = C * F;
-  constexpr int RW = CF + 1;     // record row: CF refined columns + the left column
-  constexpr int NB = 2 * F + 1;  // adjoint carry: H and G per refined row, q of the cell
+  constexpr int RW = CF + 1;      // K row of a block: CF refined columns + the left column
+  constexpr int RR = CF + 2 * F;  // record: bottom K row, left K and H per refined row
+  constexpr int NB = 2 * F + 1;   // adjoint carry: H and G per refined row, q of the cell
   constexpr T invF2 = T(1) / T(F * F);
 
+  extern __shared__ __align__(16) unsigned char dsm[];
   const int lane = threadIdx.x & 31;
+  T* ks = reinterpret_cast<T*>(dsm) + (size_t)(threadIdx.x >> 5) * F * RW * 32 + lane;
   const long long wg = (long long)blockIdx.x * WPB + (threadIdx.x >> 5);
   const long long nw = (long long)gridDim.x * WPB;
   T* scr = args.scratch + wg * args.scratch_per_warp;
   const long long steps = (long long)args.rows_max + 32;
   const long long rm = args.rows_max;
   T* REC = scr;
-  T* BL = REC + (long long)args.ns_max * steps * F * RW * 32;
+  T* BL = REC + (long long)args.ns_max * steps * RR * 32;
   T* BR = BL + 2 * rm * 2 * F;
   auto rec_at = [&](int s, long long t) {
-    return REC + ((long long)s * steps + t) * F * RW * 32 + lane;
+    return REC + ((long long)s * steps + t) * RR * 32 + lane;
   };
 
   const double alpha = 1.4426950408889634 / fmax(2.0 * args.param * args.param, 1e-12);
@@ -220,12 +233,13 @@ pde_bwd_kernel(const PdeBwdArgs<T> args) {
             }
             X[f] = kln;
             X[F + f] = H;
-            // Record refined row f: K at its lower corners, and at the
-            // column left of the lane.
-#pragma unroll
-            for (int j = 0; j < CF; ++j) rp[(f * RW + j) * 32] = Kr[j];
-            rp[(f * RW + CF) * 32] = Xin[f];
           }
+          // Record the block's boundary: its bottom K row and what came in
+          // from the left.
+#pragma unroll
+          for (int j = 0; j < CF; ++j) rp[j * 32] = Kr[j];
+#pragma unroll
+          for (int h = 0; h < 2 * F; ++h) rp[(CF + h) * 32] = Xin[h];
           kcorner = Xin[F - 1];
           if (lane == 31 && s + 1 < ns) {
 #pragma unroll
@@ -294,10 +308,63 @@ pde_bwd_kernel(const PdeBwdArgs<T> args) {
         if (act) {
           const long long t = (long long)lx + 31 - u;  // phase-1 step of this cell row
           const T* rb = rec_at(s, t);
-          const T* ra = rec_at(s, t - 1);               // the cell row above (r > 0)
+          // K row above the block: the bottom row of the cell row above
+          // (its left corner is the left K of that row's last refined row),
+          // or the boundary value 1.
+          T top[RW];
+          if (r > 0) {
+            const T* ra = rec_at(s, t - 1);
+#pragma unroll
+            for (int j = 0; j < CF; ++j) top[j] = ra[j * 32];
+            top[CF] = ra[(CF + F - 1) * 32];
+          } else {
+#pragma unroll
+            for (int j = 0; j < RW; ++j) top[j] = T(1);
+          }
+          // Rebuild the block's K rows with the forward's arithmetic.
+          {
+            T a_[C], b_[C];
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+              const T q = Z[c] * invF2;
+              b_[c] = q * q * (T(1) / T(12));
+              a_[c] = fma(T(0.5), q, b_[c]);
+            }
+            T Kr[CF];
+#pragma unroll
+            for (int j = 0; j < CF; ++j) Kr[j] = top[j];
+#pragma unroll
+            for (int f = 0; f < F; ++f) {
+              const T kin = rb[(CF + f) * 32];
+              T klo = (f == 0) ? top[CF] : rb[(CF + (f > 0 ? f - 1 : 0)) * 32];
+              T kln = kin;
+              T H = rb[(CF + F + f) * 32];
+#pragma unroll
+              for (int c = 0; c < C; ++c) {
+                const bool skip = (c == C - 1) && lane == 31;
+#pragma unroll
+                for (int g = 0; g < F; ++g) {
+                  const int J = c * F + g;
+                  const T kro = Kr[J];
+                  const T gg = fma(kro + kln, a_[c], klo * b_[c]);
+                  const T Hn = H + gg;
+                  const T krn = kro + Hn;
+                  if (!skip) {
+                    klo = kro;
+                    kln = krn;
+                    H = Hn;
+                    Kr[J] = krn;
+                  }
+                }
+              }
+#pragma unroll
+              for (int j = 0; j < CF; ++j) ks[(f * RW + j) * 32] = Kr[j];
+              ks[(f * RW + CF) * 32] = kin;
+            }
+          }
           T Kbot[RW], Ktop[RW];
 #pragma unroll
-          for (int j = 0; j < RW; ++j) Kbot[j] = rb[((F - 1) * RW + j) * 32];
+          for (int j = 0; j < RW; ++j) Kbot[j] = ks[((F - 1) * RW + j) * 32];
           T Gbel[CF], Gcur[CF];
 #pragma unroll
           for (int j = 0; j < CF; ++j) { Gbel[j] = Gb[j]; Gcur[j] = T(0); }
@@ -305,13 +372,10 @@ pde_bwd_kernel(const PdeBwdArgs<T> args) {
           for (int f = F - 1; f >= 0; --f) {
             if (f > 0) {
 #pragma unroll
-              for (int j = 0; j < RW; ++j) Ktop[j] = rb[((f > 0 ? f - 1 : 0) * RW + j) * 32];
-            } else if (r > 0) {
-#pragma unroll
-              for (int j = 0; j < RW; ++j) Ktop[j] = ra[((F - 1) * RW + j) * 32];
+              for (int j = 0; j < RW; ++j) Ktop[j] = ks[((f > 0 ? f - 1 : 0) * RW + j) * 32];
             } else {
 #pragma unroll
-              for (int j = 0; j < RW; ++j) Ktop[j] = T(1);
+              for (int j = 0; j < RW; ++j) Ktop[j] = top[j];
             }
             const bool last_f = f == F - 1;
             T H = Ain[f];
