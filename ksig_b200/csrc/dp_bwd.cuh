@@ -34,8 +34,9 @@
 //     (partial Mbar from its own cells); the per-row dX vector is summed
 //     along the lanes by __shfl_down and added once per row and strip.
 // Order 1 takes one left-to-right pass per row (the horizontal suffix of a
-// row is the lane total minus a running prefix); order p >= 2 records the
-// cell coefficients left to right and runs the adjoint right to left.
+// row is the lane total minus a running prefix); order p >= 2 keeps each
+// cell's horizontal prefixes left to right and runs the adjoint right to
+// left, rebuilding the cell coefficients from them.
 #pragma once
 
 #include "common.cuh"
@@ -97,7 +98,6 @@ dp_bwd_kernel(const DpBwdArgs<T> args) {
   constexpr int RV = RS / VN;
   using V = typename Vec<T>::type;
   constexpr int STRIP = 32 * C - 1;
-  constexpr int NCOEF = P == 1 ? 1 : 1 + (NL >= 2 ? (NL - 1) * P * P : 0);
 
   extern __shared__ __align__(16) unsigned char dsm[];
   const int lane = threadIdx.x & 31;
@@ -454,9 +454,11 @@ dp_bwd_kernel(const DpBwdArgs<T> args) {
             Zb[c] = zb;
           }
         } else {
-          // Left to right: forward state and the coefficient of z in every
-          // state of every level.
-          T coef[C][NCOEF];
+          // Left to right: forward state; keeps, per cell, the horizontal
+          // prefixes H the cell saw (NH values).  Together with the column
+          // sums (back at their values before this row) and z they give the
+          // coefficient of z in every state of every level (cf below).
+          T Hs[C][NX];
 #pragma unroll
           for (int c = 0; c < C; ++c) {
             const T z = Z[c];
@@ -467,18 +469,16 @@ dp_bwd_kernel(const DpBwdArgs<T> args) {
               for (int j = 0; j < P; ++j) Rp[i][j] = T(0);
             Rp[0][0] = z;
             T tot = z;
-            coef[c][0] = T(1);
 #pragma unroll
             for (int k = 2; k <= NL; ++k) {
               const int f = Lay::f(k), fp = Lay::f(k - 1), o = Lay::off(k);
-              const int cb = 1 + (k - 2) * P * P;
-              T Rn[P][P], cf[P][P];
+              T Rn[P][P];
 #pragma unroll
               for (int i = 0; i < P; ++i)
 #pragma unroll
-                for (int j = 0; j < P; ++j) { Rn[i][j] = T(0); cf[i][j] = T(0); }
+                for (int j = 0; j < P; ++j) Rn[i][j] = T(0);
               Ccol[o][c] -= tot;
-              cf[0][0] = H[o];
+              Hs[c][o] = H[o];
               Rn[0][0] = z * H[o];
               H[o] += Ccol[o][c];
               T lsum = Rn[0][0];
@@ -489,21 +489,17 @@ dp_bwd_kernel(const DpBwdArgs<T> args) {
 #pragma unroll
                   for (int i = 0; i < P; ++i)
                     if (i < fp) { Vs += Rp[i][rr - 1]; Us += Rp[rr - 1][i]; }
-                  const T inv = T(1) / T(rr + 1);
-                  const T zr = z * inv;
+                  const T zr = z * (T(1) / T(rr + 1));
                   Ccol[o + rr][c] -= Vs;
-                  cf[0][rr] = Ccol[o + rr][c] * inv;
                   Rn[0][rr] = zr * Ccol[o + rr][c];
-                  cf[rr][0] = H[o + rr] * inv;
+                  Hs[c][o + rr] = H[o + rr];
                   Rn[rr][0] = zr * H[o + rr];
                   H[o + rr] += Us;
                   lsum += Rn[0][rr] + Rn[rr][0];
 #pragma unroll
                   for (int ss = 1; ss < P; ++ss) {
                     if (ss < f) {
-                      const T inv2 = T(1) / T((rr + 1) * (ss + 1));
-                      cf[rr][ss] = Rp[rr - 1][ss - 1] * inv2;
-                      Rn[rr][ss] = z * inv2 * Rp[rr - 1][ss - 1];
+                      Rn[rr][ss] = z * (T(1) / T((rr + 1) * (ss + 1))) * Rp[rr - 1][ss - 1];
                       lsum += Rn[rr][ss];
                     }
                   }
@@ -513,12 +509,30 @@ dp_bwd_kernel(const DpBwdArgs<T> args) {
 #pragma unroll
               for (int i = 0; i < P; ++i)
 #pragma unroll
-                for (int j = 0; j < P; ++j) {
-                  Rp[i][j] = Rn[i][j];
-                  coef[c][cb + i * P + j] = cf[i][j];
-                }
+                for (int j = 0; j < P; ++j) Rp[i][j] = Rn[i][j];
             }
           }
+          // Coefficient of z in state (i, j) of level k at cell c:
+          //   (0,0): H;  (0,j): column sum / (j+1);  (i,0): H / (i+1);
+          //   (i,j): z / ((i+1)(j+1)) times the level-(k-1) coefficient of
+          //   (i-1, j-1)  (ksig/algorithms.py:121-138); level 1 is 1.
+          auto cf = [&](int c, int k, int i, int j) -> T {
+            const T z = Z[c];
+            T v = T(1);
+            int kk = k, ii = i, jj = j;
+#pragma unroll
+            for (int t = 0; t < P; ++t) {
+              if (ii >= 1 && jj >= 1) {
+                v *= z * (T(1) / T((ii + 1) * (jj + 1)));
+                --kk; --ii; --jj;
+              }
+            }
+            if (kk <= 1) return v;
+            const int o = Lay::off(kk);
+            if (ii == 0 && jj == 0) return v * Hs[c][o];
+            if (ii == 0) return v * Ccol[o + jj][c] * (T(1) / T(jj + 1));
+            return v * Hs[c][o + ii] * (T(1) / T(ii + 1));
+          };
           // Right to left: the adjoint, top level down.
           T Rb_next[C][P][P];
           T pendDA[P][C];
@@ -529,7 +543,6 @@ dp_bwd_kernel(const DpBwdArgs<T> args) {
             const int f = Lay::f(k);
             const int fn = (k < NL) ? Lay::f(k + 1) : 0;
             const int on = (k < NL) ? Lay::off(k + 1) : 0;
-            const int cb = 1 + (k - 2) * P * P;
             T Ab = (k < NL) ? Ain[on] : T(0);
             T Ub[P];
 #pragma unroll
@@ -565,7 +578,7 @@ dp_bwd_kernel(const DpBwdArgs<T> args) {
                 for (int i = 0; i < P; ++i)
 #pragma unroll
                   for (int j = 0; j < P; ++j)
-                    if (i < f && j < f) Zb[c] += Rb[i][j] * coef[c][cb + i * P + j];
+                    if (i < f && j < f) Zb[c] += Rb[i][j] * cf(c, k, i, j);
               }
               if (k < NL) {
                 Ab += E[on][c];
