@@ -7,6 +7,14 @@ one Gram is split).  ``all_gather`` is the only collective, and only when
 the caller asks for the assembled matrix.  Normalisation stays exact: a row
 block evaluated as ``K(X[rows], Y)`` normalises by the diagonals of both
 sides, exactly as the full ``K(X, Y)`` would (ksig/kernels.py:190-214).
+
+Gradients: when the block requires grad, the gather is the differentiable
+``torch.distributed.nn`` all-gather, whose backward sums the upstream
+gradients of every rank into the block's owner.  A rank's backward then
+yields dX for its own rows of X and its partial dY (the contribution of
+its block); :func:`allreduce_grads` sums both over the ranks, the one
+exchange step the adjoint has.  If every rank evaluates the same loss on
+the gathered matrix, scale that loss by 1 / world_size.
 """
 
 from typing import Callable, Optional, Tuple
@@ -49,8 +57,24 @@ def sharded_gram(kernel: Callable, X, Y=None, gather: bool = True,
   ny = block.shape[1]
   sizes = [shard_rows(n, world, r) for r in range(world)]
   maxrows = max(b - a for a, b in sizes)
-  padded = torch.zeros((maxrows, ny), dtype=block.dtype, device=block.device)
-  padded[:block.shape[0]] = block
-  parts = [torch.empty_like(padded) for _ in range(world)]
-  dist.all_gather(parts, padded, group=group)
+  if block.requires_grad:
+    import torch.distributed.nn.functional as dnn
+    pad = block.new_zeros((maxrows - block.shape[0], ny))
+    parts = dnn.all_gather(torch.cat([block, pad], dim=0), group=group)
+  else:
+    padded = torch.zeros((maxrows, ny), dtype=block.dtype, device=block.device)
+    padded[:block.shape[0]] = block
+    parts = [torch.empty_like(padded) for _ in range(world)]
+    dist.all_gather(parts, padded, group=group)
   return torch.cat([p[:b - a] for p, (a, b) in zip(parts, sizes)], dim=0)
+
+
+def allreduce_grads(tensors, group: Optional['dist.ProcessGroup'] = None):
+  """Sums ``t.grad`` over the ranks for every tensor that has one (after a
+  backward through :func:`sharded_gram`: dX rows live on their owners, dY
+  is split into per-rank partial sums)."""
+  if not dist.is_initialized():
+    return
+  for t in tensors:
+    if t is not None and t.grad is not None:
+      dist.all_reduce(t.grad, op=dist.ReduceOp.SUM, group=group)

@@ -72,3 +72,54 @@ def test_sharded_gram_two_ranks_gloo():
   for _, full, sym in res:
     np.testing.assert_allclose(full, ref, rtol=1e-12)
     np.testing.assert_allclose(sym, refx, rtol=1e-12)
+
+
+def _grad_worker(rank, world, port, X, Y, W, out_q):
+  import sys
+  sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+  from oracle import ksig_oracle_torch as OT
+  from ksig_b200.distributed import allreduce_grads, sharded_gram
+  os.environ['MASTER_ADDR'] = '127.0.0.1'
+  os.environ['MASTER_PORT'] = str(port)
+  dist.init_process_group('gloo', rank=rank, world_size=world)
+  try:
+    Xt = torch.tensor(X, requires_grad=True)
+    Yt = torch.tensor(Y, requires_grad=True)
+
+    def kern(a, b):
+      return OT.signature_kernel(list(a), list(b), n_levels=3, normalize=True, param=0.7)
+
+    full = sharded_gram(kern, Xt, Yt, gather=True)
+    ((full * torch.tensor(W)).sum() / world).backward()
+    allreduce_grads([Xt, Yt])
+    out_q.put((rank, full.detach().numpy(), Xt.grad.numpy(), Yt.grad.numpy()))
+  finally:
+    dist.destroy_process_group()
+
+
+def test_sharded_gram_gradients_two_ranks_gloo():
+  """The differentiable gather plus the gradient all-reduce give every rank
+  the unsharded dX and dY."""
+  from oracle import ksig_oracle_torch as OT
+  rng = np.random.default_rng(1)
+  X = np.cumsum(rng.standard_normal((5, 7, 2)) * 0.3, axis=1)
+  Y = np.cumsum(rng.standard_normal((3, 6, 2)) * 0.3, axis=1)
+  W = rng.standard_normal((5, 3))
+  ctx = mp.get_context('spawn')
+  q = ctx.Queue()
+  port = _free_port()
+  procs = [ctx.Process(target=_grad_worker, args=(r, 2, port, X, Y, W, q)) for r in range(2)]
+  for p in procs:
+    p.start()
+  res = [q.get(timeout=180) for _ in procs]
+  for p in procs:
+    p.join(timeout=60)
+    assert p.exitcode == 0
+  Xt = torch.tensor(X, requires_grad=True)
+  Yt = torch.tensor(Y, requires_grad=True)
+  ref = OT.signature_kernel(list(Xt), list(Yt), n_levels=3, normalize=True, param=0.7)
+  (ref * torch.tensor(W)).sum().backward()
+  for _, full, gx, gy in res:
+    np.testing.assert_allclose(full, ref.detach().numpy(), rtol=1e-12)
+    np.testing.assert_allclose(gx, Xt.grad.numpy(), rtol=1e-10, atol=1e-14)
+    np.testing.assert_allclose(gy, Yt.grad.numpy(), rtol=1e-10, atol=1e-14)
