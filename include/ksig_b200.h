@@ -51,9 +51,17 @@ extern "C" {
 #define KSIG_ERR_DEVICE 5      /* device-side check failed (bounded wait,
                                   bounds check); the context stays usable    */
 
-/* Static (state-space) kernels. */
-#define KSIG_STATIC_RBF 0    /* exp(-|x-y|^2 / max(2 param^2, 1e-12))  */
-#define KSIG_STATIC_LINEAR 1 /* param * <x, y>                          */
+/* Static (state-space) kernels.  The *_ex entry points take the parameter
+ * list shown in braces (ksig/static/kernels.py:137-343); the others take
+ * the one parameter of RBF and linear. */
+#define KSIG_STATIC_RBF 0       /* {s}: exp(-|x-y|^2 / max(2 s^2, 1e-12))        */
+#define KSIG_STATIC_LINEAR 1    /* {s}: s <x, y>                                  */
+#define KSIG_STATIC_POLY 2      /* {degree, gamma, scale}:
+                                   scale (<x, y> + gamma)^degree                 */
+#define KSIG_STATIC_MATERN12 3  /* {s}: exp(-D), D = |x-y| / s                   */
+#define KSIG_STATIC_MATERN32 4  /* {s}: (1 + D) exp(-D), D = sqrt(3) |x-y| / s   */
+#define KSIG_STATIC_MATERN52 5  /* {s}: (1 + D + D^2/3) exp(-D), D = sqrt(5) |x-y| / s */
+#define KSIG_STATIC_RQ 6        /* {s, a}: (1 + |x-y|^2 / (2 a s^2))^-a           */
 
 /* Element types. */
 #define KSIG_DTYPE_F32 0
@@ -195,6 +203,30 @@ int ksig_signature_kern_pde(const void* X, const int32_t* lenX, int nX,
                             const int32_t* pair_list, int n_list,
                             double* out, void* workspace,
                             size_t workspace_bytes, void* stream);
+
+/*
+ * ksig_signature_kern and ksig_signature_kern_pde for every static kernel
+ * of ksig.static.kernels: `static_params` holds the kind's parameters as
+ * listed with KSIG_STATIC_* (up to 3 values; positive where the reference
+ * requires it, ksig/utils.py:23-35).  Same workspace as the plain entry
+ * points.  The adjoint entry points support RBF and linear only.
+ */
+int ksig_signature_kern_ex(const void* X, const int32_t* lenX, int nX, int LX,
+                           const void* Y, const int32_t* lenY, int nY, int LY,
+                           int d, int dtype, int static_kind,
+                           const double* static_params, int n_levels,
+                           int order, int difference, int pairs_mode,
+                           const int32_t* pair_list, int n_list,
+                           double* out_levels, void* workspace,
+                           size_t workspace_bytes, void* stream);
+int ksig_signature_kern_pde_ex(const void* X, const int32_t* lenX, int nX,
+                               int LX, const void* Y, const int32_t* lenY,
+                               int nY, int LY, int d, int dtype,
+                               int static_kind, const double* static_params,
+                               int dyadic_order, int difference,
+                               int pairs_mode, const int32_t* pair_list,
+                               int n_list, double* out, void* workspace,
+                               size_t workspace_bytes, void* stream);
 
 /* Workspace (bytes) required by ksig_signature_kern_bwd. */
 size_t ksig_signature_kern_bwd_workspace(int nX, int LX, int nY, int LY,

@@ -6,12 +6,15 @@ Importing the package does not touch the GPU; the CUDA library
 
 from . import graphs  # noqa: F401
 from . import kernels  # noqa: F401
+from . import precompute  # noqa: F401
 from . import static  # noqa: F401
 from . import tuning  # noqa: F401
 from . import utils  # noqa: F401
 from .graphs import GraphedKernel  # noqa: F401
 from .kernels import Ragged, SignatureKernel, SignaturePDEKernel  # noqa: F401
-from .static.kernels import LinearKernel, RBFKernel  # noqa: F401
+from .static.kernels import (LinearKernel, Matern12Kernel, Matern32Kernel,  # noqa: F401
+                             Matern52Kernel, PolynomialKernel, RationalQuadraticKernel,
+                             RBFKernel)
 
 from ._engine import check_device_status  # noqa: F401
 

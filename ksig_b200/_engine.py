@@ -82,6 +82,17 @@ def num_pairs(mode, nX, nY, n_list=0):
   return int(L.lib().ksig_num_pairs(mode, nX, nY, n_list))
 
 
+def _static_args(kind, param):
+  """(use_ex, float param, ctypes double[3]) for a static kernel given as
+  one parameter (RBF, linear) or a parameter tuple (every kind)."""
+  if isinstance(param, (tuple, list)):
+    vals = [float(v) for v in param] + [0.0] * (3 - len(param))
+    return True, vals[0], (ctypes.c_double * 3)(*vals[:3])
+  if kind not in (L.STATIC_RBF, L.STATIC_LINEAR):
+    raise ValueError('this static kernel needs its parameter tuple')
+  return False, float(param), None
+
+
 def sig_levels(X, Y, mode, n_levels, order, difference, kind, param,
                pair_list=None):
   """Per-level signature kernels ``[n_levels+1, P]`` (float64)."""
@@ -103,11 +114,19 @@ def sig_levels(X, Y, mode, n_levels, order, difference, kind, param,
     L.check(L.ERR_UNSUPPORTED if 'no compiled' in L.last_error()
             else L.ERR_INVALID)
   ws = _workspace(ws_bytes, X.data.device)
-  rc = lib.ksig_signature_kern(
-      _ptr(X.data), _ptr(X.lengths), X.n, X.L, _ptr(Yv.data),
-      _ptr(Yv.lengths), Yv.n, Yv.L, X.d, dt, kind, float(param), n_levels,
-      order, int(difference), mode, _ptr(pair_list), n_list, _ptr(out),
-      _ptr(ws), ws_bytes, _stream())
+  ext, p0, pv = _static_args(kind, param)
+  if ext:
+    rc = lib.ksig_signature_kern_ex(
+        _ptr(X.data), _ptr(X.lengths), X.n, X.L, _ptr(Yv.data),
+        _ptr(Yv.lengths), Yv.n, Yv.L, X.d, dt, kind, pv, n_levels,
+        order, int(difference), mode, _ptr(pair_list), n_list, _ptr(out),
+        _ptr(ws), ws_bytes, _stream())
+  else:
+    rc = lib.ksig_signature_kern(
+        _ptr(X.data), _ptr(X.lengths), X.n, X.L, _ptr(Yv.data),
+        _ptr(Yv.lengths), Yv.n, Yv.L, X.d, dt, kind, p0, n_levels,
+        order, int(difference), mode, _ptr(pair_list), n_list, _ptr(out),
+        _ptr(ws), ws_bytes, _stream())
   L.check(rc)
   _fold_status(ws)
   return out
@@ -217,11 +236,19 @@ def pde_values(X, Y, mode, dyadic_order, difference, kind, param,
     L.check(L.ERR_UNSUPPORTED if 'no compiled' in L.last_error()
             else L.ERR_INVALID)
   ws = _workspace(ws_bytes, X.data.device)
-  rc = lib.ksig_signature_kern_pde(
-      _ptr(X.data), _ptr(X.lengths), X.n, X.L, _ptr(Yv.data),
-      _ptr(Yv.lengths), Yv.n, Yv.L, X.d, dt, kind, float(param),
-      dyadic_order, int(difference), mode, _ptr(pair_list), n_list,
-      _ptr(out), _ptr(ws), ws_bytes, _stream())
+  ext, p0, pv = _static_args(kind, param)
+  if ext:
+    rc = lib.ksig_signature_kern_pde_ex(
+        _ptr(X.data), _ptr(X.lengths), X.n, X.L, _ptr(Yv.data),
+        _ptr(Yv.lengths), Yv.n, Yv.L, X.d, dt, kind, pv,
+        dyadic_order, int(difference), mode, _ptr(pair_list), n_list,
+        _ptr(out), _ptr(ws), ws_bytes, _stream())
+  else:
+    rc = lib.ksig_signature_kern_pde(
+        _ptr(X.data), _ptr(X.lengths), X.n, X.L, _ptr(Yv.data),
+        _ptr(Yv.lengths), Yv.n, Yv.L, X.d, dt, kind, p0,
+        dyadic_order, int(difference), mode, _ptr(pair_list), n_list,
+        _ptr(out), _ptr(ws), ws_bytes, _stream())
   L.check(rc)
   _fold_status(ws)
   return out

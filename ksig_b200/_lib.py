@@ -21,6 +21,11 @@ ERR_DEVICE = 5
 
 STATIC_RBF = 0
 STATIC_LINEAR = 1
+STATIC_POLY = 2
+STATIC_MATERN12 = 3
+STATIC_MATERN32 = 4
+STATIC_MATERN52 = 5
+STATIC_RQ = 6
 DTYPE_F32 = 0
 DTYPE_F64 = 1
 PAIRS_FULL = 0
@@ -69,6 +74,12 @@ _SIGNATURES = {
                                            _P, _P, _P, _SZ, _P]),
     'ksig_tune_set_cols': (_I, [_I, _I]),
     'ksig_tune_get_cols': (_I, [_I]),
+    'ksig_signature_kern_ex': (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _I, _I,
+                                    _I, _P, _I, _I, _I, _I, _P, _I, _P, _P,
+                                    _SZ, _P]),
+    'ksig_signature_kern_pde_ex': (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _I,
+                                        _I, _I, _P, _I, _I, _I, _P, _I, _P,
+                                        _P, _SZ, _P]),
     'ksig_launch_count': (ctypes.c_ulonglong, []),
     'ksig_profile_enable': (None, [_I]),
     'ksig_profile_read': (_I, [ctypes.POINTER(ctypes.c_double),

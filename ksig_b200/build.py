@@ -75,6 +75,14 @@ def instances():
   for dt in ('f32', 'f64'):
     for f, kd in itertools.product([1, 2, 4], KD_FEW):
       add(('pde', dt, kd, 2, 0, f, 0))
+  # Forward sweeps for the other static kernels (polynomial, Matern,
+  # rational quadratic): one tile width per dtype.
+  for dt, c in (('f32', 4), ('f64', 2)):
+    for p, nls in ((1, NL_ALL), (2, [2, 3, 4, 5, 6, 8])):
+      for nl, kd in itertools.product(nls, KD_FEW):
+        add(('dpx', dt, kd, c, nl, p, 1))
+    for f, kd in itertools.product([1, 2, 4, 8], KD_FEW):
+      add(('pdex', dt, kd, c, 0, f, 1))
   # PDE backward (row-side gradients).
   for f, kd, c in itertools.product([1, 2, 4, 8], KD_MID, [2, 4, 8]):
     if c * f <= 16:  # the adjoint keeps three C*F-wide rows in registers
@@ -94,8 +102,10 @@ def instances():
 
 
 OPS = {
-    'dp': ('OP_DP_FWD', 'dp_fwd_kernel<{T}, {kd}, {c}, {nl}, {p}, {diff}, {wpb}>'),
-    'pde': ('OP_PDE_FWD', 'pde_fwd_kernel<{T}, {kd}, {c}, {p}, {diff}, {wpb}>'),
+    'dp': ('OP_DP_FWD', 'dp_fwd_kernel<{T}, {kd}, {c}, {nl}, {p}, {diff}, {wpb}, false>'),
+    'pde': ('OP_PDE_FWD', 'pde_fwd_kernel<{T}, {kd}, {c}, {p}, {diff}, {wpb}, false>'),
+    'dpx': ('OP_DP_FWD_EXT', 'dp_fwd_kernel<{T}, {kd}, {c}, {nl}, {p}, {diff}, {wpb}, true>'),
+    'pdex': ('OP_PDE_FWD_EXT', 'pde_fwd_kernel<{T}, {kd}, {c}, {p}, {diff}, {wpb}, true>'),
     'dpb': ('OP_DP_BWD', 'dp_bwd_kernel<{T}, {kd}, {c}, {nl}, {p}, {wpb}>'),
     'pdeb': ('OP_PDE_BWD', 'pde_bwd_kernel<{T}, {kd}, {c}, {p}, {wpb}>'),
 }

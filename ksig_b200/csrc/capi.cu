@@ -302,7 +302,7 @@ int want_cols(int ly_cells, int cap, int op) {
 
 int plan_fwd(bool pde, int nX, int LX, int nY, int LY, int d, int dtype, int n_levels,
              int order_or_dyadic, int difference, int pairs_mode, int n_list,
-             FwdPlan& pl, bool allow_order = true) {
+             FwdPlan& pl, bool allow_order = true, bool ext = false) {
   if (dtype != KSIG_DTYPE_F32 && dtype != KSIG_DTYPE_F64)
     return fail(KSIG_ERR_INVALID, "dtype must be KSIG_DTYPE_F32 or KSIG_DTYPE_F64");
   if (nX <= 0 || LX <= 0 || d <= 0) return fail(KSIG_ERR_INVALID, "empty X (n=%d, L=%d, d=%d)", nX, LX, d);
@@ -330,13 +330,14 @@ int plan_fwd(bool pde, int nX, int LX, int nY, int LY, int d, int dtype, int n_l
   }
   const int ly_cells = pl.diff ? LY - 1 : LY;
   const int lx_cells = pl.diff ? LX - 1 : LX;
-  const int op = pde ? OP_PDE_FWD : OP_DP_FWD;
+  const int op = ext ? (pde ? OP_PDE_FWD_EXT : OP_DP_FWD_EXT) : (pde ? OP_PDE_FWD : OP_DP_FWD);
   const int want = want_cols(ly_cells, 8, op);
   const KernelEntry* k = find_kernel(op, pl.f64, d, want, need_nl, p, pl.diff);
   if (!k)
     return fail(KSIG_ERR_UNSUPPORTED,
-                "no compiled %s kernel for dtype=%s d=%d n_levels=%d order/F=%d difference=%d",
-                pde ? "PDE" : "DP", pl.f64 ? "f64" : "f32", d, n_levels, p, pl.diff);
+                "no compiled %s kernel for dtype=%s d=%d n_levels=%d order/F=%d difference=%d%s",
+                pde ? "PDE" : "DP", pl.f64 ? "f64" : "f32", d, n_levels, p, pl.diff,
+                ext ? " (polynomial / Matern / rational quadratic static kernel)" : "");
   pl.k = k;
   pl.kd = k->kd;
   pl.c = k->c;
@@ -407,7 +408,8 @@ int pack(const void* src, const int32_t* len, int n, int L, int d, int src_f64, 
 template <typename T>
 int run_fwd(const FwdPlan& pl, const void* X, const int32_t* lenX, int nX, int LX, const void* Y,
             const int32_t* lenY, int nY, int LY, int d, int src_f64, int kind, double param,
-            int mode, const int32_t* list, double* out, char* ws, cudaStream_t st) {
+            const StaticParams& sp, int mode, const int32_t* list, double* out, char* ws,
+            cudaStream_t st) {
   int* status = reinterpret_cast<int*>(ws + pl.off_status);
   T* xr = reinterpret_cast<T*>(ws + pl.off_xr);
   T* yr = reinterpret_cast<T*>(ws + pl.off_yr);
@@ -432,6 +434,7 @@ int run_fwd(const FwdPlan& pl, const void* X, const int32_t* lenX, int nX, int L
   if (rc) return rc;
   a.ntasks = (int)pl.ntasks;
   a.kind = kind;
+  a.sp = sp;
   a.out = out;
   a.scratch = pl.multi ? reinterpret_cast<T*>(ws + pl.off_scratch) : nullptr;
   a.scratch_per_warp = pl.scratch_per_warp;
@@ -829,6 +832,42 @@ int run_plain_bwd(const PlainBwdPlan& bp, const void* X, const int32_t* lenX, in
   return KSIG_OK;
 }
 
+// Validates the parameters of any static kernel kind (ksig/utils.py:23-35
+// messages) and forms its epilogue constants (common.cuh, static_value).
+int static_params(int kind, const double* p, StaticParams& sp) {
+  const double eps = 1e-12;
+  auto positive = [&](double v, const char* name) {
+    if (!(v > 0))
+      return fail(KSIG_ERR_INVALID, "The parameter '%s' should have a positive value.", name);
+    return (int)KSIG_OK;
+  };
+  sp = StaticParams{0.0, 0.0, 0.0};
+  int rc = KSIG_OK;
+  switch (kind) {
+    case KSIG_STATIC_RBF: return positive(p[0], "bandwidth");
+    case KSIG_STATIC_LINEAR: return positive(p[0], "scale");
+    case KSIG_STATIC_POLY:
+      if ((rc = positive(p[0], "degree")) || (rc = positive(p[2], "scale"))) return rc;
+      sp = StaticParams{p[1], p[0], p[2]};
+      return KSIG_OK;
+    case KSIG_STATIC_MATERN12:
+    case KSIG_STATIC_MATERN32:
+      if ((rc = positive(p[0], "bandwidth"))) return rc;
+      sp.c0 = (kind == KSIG_STATIC_MATERN32 ? sqrt(3.0) : 1.0) / fmax(p[0], eps);
+      return KSIG_OK;
+    case KSIG_STATIC_MATERN52:
+      if ((rc = positive(p[0], "bandwidth"))) return rc;
+      sp.c0 = 5.0 / fmax(p[0] * p[0], eps);
+      return KSIG_OK;
+    case KSIG_STATIC_RQ:
+      if ((rc = positive(p[0], "bandwidth")) || (rc = positive(p[1], "alpha"))) return rc;
+      sp.c0 = 1.0 / fmax(2.0 * p[1] * p[0] * p[0], eps);
+      sp.c1 = p[1];
+      return KSIG_OK;
+  }
+  return fail(KSIG_ERR_INVALID, "unknown static kernel %d", kind);
+}
+
 int check_common(const void* X, const void* Y, int pairs_mode, const int32_t* list, int n_list,
                  int static_kind, double static_param) {
   if (!X) return fail(KSIG_ERR_INVALID, "X is NULL");
@@ -848,13 +887,25 @@ int fwd_entry(bool pde, const void* X, const int32_t* lenX, int nX, int LX, cons
               const int32_t* lenY, int nY, int LY, int d, int dtype, int static_kind,
               double static_param, int n_levels, int order_or_dyadic, int difference,
               int pairs_mode, const int32_t* list, int n_list, double* out, void* ws,
-              size_t ws_bytes, void* stream, bool allow_order = true) {
-  int rc = check_common(X, Y, pairs_mode, list, n_list, static_kind, static_param);
+              size_t ws_bytes, void* stream, bool allow_order = true,
+              const double* ext_params = nullptr) {
+  // ext_params: the *_ex entry points' parameter list (any static kernel);
+  // otherwise RBF / linear with static_param.
+  StaticParams sp{0.0, 0.0, 0.0};
+  int rc;
+  if (ext_params) {
+    rc = check_common(X, Y, pairs_mode, list, n_list, KSIG_STATIC_RBF, 1.0);
+    if (!rc) rc = static_params(static_kind, ext_params, sp);
+    static_param = ext_params[0];
+  } else {
+    rc = check_common(X, Y, pairs_mode, list, n_list, static_kind, static_param);
+  }
   if (rc) return rc;
   if (!out) return fail(KSIG_ERR_INVALID, "output is NULL");
   FwdPlan pl;
+  const bool ext = static_kind != KSIG_STATIC_RBF && static_kind != KSIG_STATIC_LINEAR;
   rc = plan_fwd(pde, nX, LX, nY, LY, d, dtype, n_levels, order_or_dyadic, difference, pairs_mode,
-                n_list, pl, allow_order);
+                n_list, pl, allow_order, ext);
   if (rc) return rc;
   if (!ws || ws_bytes < pl.total)
     return fail(KSIG_ERR_WORKSPACE, "workspace of %zu bytes is smaller than the %zu required",
@@ -865,9 +916,9 @@ int fwd_entry(bool pde, const void* X, const int32_t* lenX, int nX, int LX, cons
   if (pairs_mode == KSIG_PAIRS_UPPER || pairs_mode == KSIG_PAIRS_DIAG) { nY = nX; LY = LX; Y = X; lenY = lenX; }
   const int f64 = dtype == KSIG_DTYPE_F64;
   if (f64)
-    return run_fwd<double>(pl, X, lenX, nX, LX, Y, lenY, nY, LY, d, 1, static_kind, static_param,
+    return run_fwd<double>(pl, X, lenX, nX, LX, Y, lenY, nY, LY, d, 1, static_kind, static_param, sp,
                            pairs_mode, list, out, static_cast<char*>(ws), st);
-  return run_fwd<float>(pl, X, lenX, nX, LX, Y, lenY, nY, LY, d, 0, static_kind, static_param,
+  return run_fwd<float>(pl, X, lenX, nX, LX, Y, lenY, nY, LY, d, 0, static_kind, static_param, sp,
                         pairs_mode, list, out, static_cast<char*>(ws), st);
 }
 
@@ -955,6 +1006,13 @@ size_t ksig_signature_kern_workspace(int nX, int LX, int nY, int LY, int d, int 
   if (plan_fwd(false, nX, LX, nY, LY, d, dtype, n_levels, order, difference, pairs_mode, n_list,
                pl))
     return 0;
+  // Also large enough for the other static kernels' instantiations
+  // (ksig_signature_kern_ex), where one is compiled for this shape.
+  FwdPlan px;
+  if (!plan_fwd(false, nX, LX, nY, LY, d, dtype, n_levels, order, difference, pairs_mode, n_list,
+                px, true, true) &&
+      px.total > pl.total)
+    return px.total;
   return pl.total;
 }
 
@@ -975,6 +1033,11 @@ size_t ksig_signature_kern_pde_workspace(int nX, int LX, int nY, int LY, int d, 
   if (plan_fwd(true, nX, LX, nY, LY, d, dtype, 0, dyadic_order, difference, pairs_mode, n_list,
                pl))
     return 0;
+  FwdPlan px;
+  if (!plan_fwd(true, nX, LX, nY, LY, d, dtype, 0, dyadic_order, difference, pairs_mode, n_list,
+                px, true, true) &&
+      px.total > pl.total)
+    return px.total;
   return pl.total;
 }
 
@@ -986,6 +1049,30 @@ int ksig_signature_kern_pde(const void* X, const int32_t* lenX, int nX, int LX, 
   return fwd_entry(true, X, lenX, nX, LX, Y, lenY, nY, LY, d, dtype, static_kind, static_param,
                    0, dyadic_order, difference, pairs_mode, pair_list, n_list, out, workspace,
                    workspace_bytes, stream);
+}
+
+int ksig_signature_kern_ex(const void* X, const int32_t* lenX, int nX, int LX, const void* Y,
+                           const int32_t* lenY, int nY, int LY, int d, int dtype,
+                           int static_kind, const double* static_params, int n_levels, int order,
+                           int difference, int pairs_mode, const int32_t* pair_list, int n_list,
+                           double* out_levels, void* workspace, size_t workspace_bytes,
+                           void* stream) {
+  if (!static_params) return fail(KSIG_ERR_INVALID, "static_params is NULL");
+  return fwd_entry(false, X, lenX, nX, LX, Y, lenY, nY, LY, d, dtype, static_kind,
+                   static_params[0], n_levels, order, difference, pairs_mode, pair_list, n_list,
+                   out_levels, workspace, workspace_bytes, stream, true, static_params);
+}
+
+int ksig_signature_kern_pde_ex(const void* X, const int32_t* lenX, int nX, int LX,
+                               const void* Y, const int32_t* lenY, int nY, int LY, int d,
+                               int dtype, int static_kind, const double* static_params,
+                               int dyadic_order, int difference, int pairs_mode,
+                               const int32_t* pair_list, int n_list, double* out,
+                               void* workspace, size_t workspace_bytes, void* stream) {
+  if (!static_params) return fail(KSIG_ERR_INVALID, "static_params is NULL");
+  return fwd_entry(true, X, lenX, nX, LX, Y, lenY, nY, LY, d, dtype, static_kind,
+                   static_params[0], 0, dyadic_order, difference, pairs_mode, pair_list, n_list,
+                   out, workspace, workspace_bytes, stream, true, static_params);
 }
 
 int ksig_signature_kern_static(const void* X, const int32_t* lenX, int nX, int LX,

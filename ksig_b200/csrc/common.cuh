@@ -12,7 +12,27 @@ constexpr unsigned FULL = 0xffffffffu;
 
 // Static-kernel epilogue selector (ksig/static/kernels.py:245-260 RBF,
 // :134-155 linear).
-enum StaticKind : int { KIND_RBF = KSIG_STATIC_RBF, KIND_LINEAR = KSIG_STATIC_LINEAR };
+enum StaticKind : int {
+  KIND_RBF = KSIG_STATIC_RBF,
+  KIND_LINEAR = KSIG_STATIC_LINEAR,
+  KIND_POLY = KSIG_STATIC_POLY,            // ksig/static/kernels.py:183-194
+  KIND_MATERN12 = KSIG_STATIC_MATERN12,    // :263-277
+  KIND_MATERN32 = KSIG_STATIC_MATERN32,    // :280-296
+  KIND_MATERN52 = KSIG_STATIC_MATERN52,    // :299-316
+  KIND_RQ = KSIG_STATIC_RQ,                // :319-343
+};
+
+// Kernels whose packed argument is minus the squared distance.
+__host__ __device__ inline bool kind_is_distance(int kind) {
+  return kind == KIND_RBF || kind == KIND_MATERN12 || kind == KIND_MATERN32 ||
+         kind == KIND_MATERN52 || kind == KIND_RQ;
+}
+
+// Epilogue constants of a static kernel, formed on the host (capi.cu,
+// static_params).
+struct StaticParams {
+  double c0, c1, c2;
+};
 
 // Device-side status word: kernels never trap; they record the first error
 // code here and return.  The host reads it after the launch.
@@ -28,10 +48,44 @@ template <> struct Vec<double> { using type = double2; static constexpr int N = 
 __device__ __forceinline__ float kexp2(float a) { return exp2f(a); }
 __device__ __forceinline__ double kexp2(double a) { return exp2(a); }
 
-// Static kernel value from the fused dot-product argument.
+// Static kernel value from the fused dot-product argument (RBF, linear).
 template <typename T>
 __device__ __forceinline__ T static_value(T arg, int kind) {
   return kind == KIND_RBF ? kexp2(arg) : arg;
+}
+
+// Static kernel values of the other kinds, evaluated by their own sweep
+// instantiations (EXT = true).  `arg` is <x, y> for the polynomial kernel
+// and minus the squared distance D2 = |x-y|^2 for the others:
+//   polynomial  c2 (arg + c0)^c1                  (scale, gamma, degree)
+//   Matern12    exp(-D),  D = sqrt(max(D2, 1e-12)) c0,  c0 = 1 / max(s, eps)
+//   Matern32    (1 + D) exp(-D),  same D with c0 = sqrt(3) / max(s, eps)
+//   Matern52    (1 + D + E/3) exp(-D),  E = c0 D2, D = sqrt(max(E, 1e-12)),
+//               c0 = 5 / max(s^2, eps)
+//   RQ          (1 + c0 D2)^-c1,  c0 = 1 / max(2 a s^2, eps), c1 = a
+// Matern12 / 32 use the distance between x and y; the reference's
+// euclid_dist (ksig/utils.py:186-197) takes a stray `self` argument and
+// measures within the second set instead, which this does not reproduce.
+template <typename T>
+__device__ __forceinline__ T static_value_other(T arg, int kind, const StaticParams& sp) {
+  switch (kind) {
+    case KIND_POLY: return T(sp.c2) * pow(arg + T(sp.c0), T(sp.c1));
+    case KIND_MATERN12: {
+      const T D = sqrt(fmax(-arg, T(1e-12))) * T(sp.c0);
+      return exp(-D);
+    }
+    case KIND_MATERN32: {
+      const T D = sqrt(fmax(-arg, T(1e-12))) * T(sp.c0);
+      return (T(1) + D) * exp(-D);
+    }
+    case KIND_MATERN52: {
+      const T E = -arg * T(sp.c0);
+      const T D = sqrt(fmax(E, T(1e-12)));
+      return (T(1) + D + E * (T(1) / T(3))) * exp(-D);
+    }
+    case KIND_RQ: return pow(T(1) + (-arg) * T(sp.c0), -T(sp.c1));
+    default: return arg;
+  }
 }
 
 template <typename T>

@@ -7,6 +7,9 @@
 //          xr = (2a x, -a|x|^2), yr = (y, -a|y|^2), a = log2(e)/max(2s^2,1e-12)
 //          so arg = -a |x-y|^2 and M = exp2(arg) = exp(-|x-y|^2 / max(2s^2,eps)).
 //   linear (ksig/static/kernels.py:155): xr = (s x, 0), yr = (y, 0), M = arg.
+//   polynomial: as linear with s = 1 (arg = <x, y>); Matern / rational
+//          quadratic: as RBF with a = 1 (arg = -|x-y|^2); the kernel value
+//          is formed by static_value (common.cuh).
 // Rows are padded with zeros to KD coordinates and to a 16-byte stride so the
 // kernels read them with vector loads.  Norms are formed in FP64.
 #pragma once
@@ -32,7 +35,10 @@ struct PackArgs {
 template <typename T>
 __global__ void pack_rows_kernel(PackArgs a, T* __restrict__ dst) {
   const long long total = (long long)a.n * a.L;
-  const double alpha = 1.4426950408889634 / fmax(2.0 * a.param * a.param, 1e-12);
+  const bool dist = kind_is_distance(a.kind);
+  const double alpha =
+      a.kind == KIND_RBF ? 1.4426950408889634 / fmax(2.0 * a.param * a.param, 1e-12) : 1.0;
+  const double lin = a.kind == KIND_LINEAR ? a.param : 1.0;
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < total;
        r += (long long)gridDim.x * blockDim.x) {
     const int seq = (int)(r / a.L);
@@ -52,11 +58,11 @@ __global__ void pack_rows_kernel(PackArgs a, T* __restrict__ dst) {
       }
       nrm += v * v;
       double o;
-      if (a.kind == KIND_RBF) o = a.row_side ? 2.0 * alpha * v : v;
-      else o = a.row_side ? a.param * v : v;
+      if (dist) o = a.row_side ? 2.0 * alpha * v : v;
+      else o = a.row_side ? lin * v : v;
       out[k] = (T)o;
     }
-    out[a.kd] = (T)(a.kind == KIND_RBF ? -alpha * nrm : 0.0);
+    out[a.kd] = (T)(dist ? -alpha * nrm : 0.0);
     for (int k = a.kd + 1; k < a.stride; ++k) out[k] = (T)0;
   }
 }

@@ -11,6 +11,8 @@ enum KernelOp : int {
   OP_PDE_FWD = 1,  // SweepArgs<T>          pde_fwd_kernel   (p = refinement F)
   OP_DP_BWD = 2,   // DpBwdArgs<T>          dp_bwd_kernel
   OP_PDE_BWD = 3,  // PdeBwdArgs<T>         pde_bwd_kernel
+  OP_DP_FWD_EXT = 4,   // dp_fwd_kernel, EXT: the other static kernels
+  OP_PDE_FWD_EXT = 5,  // pde_fwd_kernel, EXT
 };
 
 struct KernelEntry {

@@ -55,6 +55,7 @@ struct SweepArgs {
   int nl_out;            // levels written (<= the instantiated NL)
   int nX, nYseq;         // sequence counts (bounds of LIST pairs)
   int* status;
+  StaticParams sp;       // epilogue constants of the other static kernels (EXT)
 };
 
 // Item geometry a policy may need.
@@ -71,7 +72,7 @@ struct SweepSmem {
   T ynext[32][C * RS];
 };
 
-template <typename T, int KD, int C, bool DIFF, int WPB, class Policy>
+template <typename T, int KD, int C, bool DIFF, int WPB, bool EXT, class Policy>
 __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
                                       SweepSmem<T, KD, C>& sm) {
   constexpr int NX = Policy::NX;
@@ -173,14 +174,34 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
       m[c] = RBF ? kexp2(acc) : acc;
     }
   };
-  // Runtime-kind version for the rare paths (one copy of the code).
+  // Runtime-kind version for the rare paths (one copy of the code).  The
+  // EXT instantiations serve the other static kernels: the squared
+  // distance is summed from coordinate differences (row points are packed
+  // as 2x, so x is exact), which keeps it accurate for nearby points where
+  // |x|^2 + |y|^2 - 2<x,y> would cancel (the Matern kernels have a cusp
+  // there).
   auto gram_rt = [&](const T (&xv)[RS], T (&m)[C]) {
 #pragma unroll
     for (int c = 0; c < C; ++c) {
-      T acc = xv[KD] + yv[c][KD];
+      if constexpr (EXT) {
+        T acc = T(0);
+        if (args.kind == KIND_POLY) {
 #pragma unroll
-      for (int k = 0; k < KD; ++k) acc = fma(xv[k], yv[c][k], acc);
-      m[c] = static_value(acc, args.kind);
+          for (int k = 0; k < KD; ++k) acc = fma(xv[k], yv[c][k], acc);
+        } else {
+#pragma unroll
+          for (int k = 0; k < KD; ++k) {
+            const T dk = fma(T(0.5), xv[k], -yv[c][k]);
+            acc = fma(-dk, dk, acc);
+          }
+        }
+        m[c] = static_value_other(acc, args.kind, args.sp);
+      } else {
+        T acc = xv[KD] + yv[c][KD];
+#pragma unroll
+        for (int k = 0; k < KD; ++k) acc = fma(xv[k], yv[c][k], acc);
+        m[c] = static_value(acc, args.kind);
+      }
     }
   };
 
@@ -207,6 +228,7 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
   stage_y(nxt);
 
   const bool rbf = args.kind == KIND_RBF;
+  const bool fast = !EXT && (rbf || args.kind == KIND_LINEAR);
   T Mcur[C], DMcur[C], Mtmp[C], DMtmp[C];
   T xv[RS];
   load_x(cur.xb, cur.Lx, 0, xv);
@@ -350,7 +372,9 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
     // last step (u < rows); then no item switch, no begin/end hook and no
     // pair completion happens, and every lane has a recorded row.
     {
-      const bool plain = delay == 0 && !done && u >= 3 && u < cur.rows;
+      // (RBF and linear only: the other static kernels take the general
+      // step with the run-time epilogue.)
+      const bool plain = fast && delay == 0 && !done && u >= 3 && u < cur.rows;
       const int nplain = __reduce_min_sync(FULL, plain ? cur.rows - u : 0);
       if (nplain > 0) {
         if (rbf) steady_run(1, nplain);
@@ -626,7 +650,7 @@ struct DpPolicy {
   }
 };
 
-template <typename T, int KD, int C, int NL, int P, bool DIFF, int WPB>
+template <typename T, int KD, int C, int NL, int P, bool DIFF, int WPB, bool EXT>
 __global__ void __launch_bounds__(WPB * 32)
 dp_fwd_kernel(const SweepArgs<T> args) {
   __shared__ double red[WPB][2][NL][32];
@@ -634,7 +658,7 @@ dp_fwd_kernel(const SweepArgs<T> args) {
   auto* sm = reinterpret_cast<SweepSmem<T, KD, C>*>(dyn_smem);
   DpPolicy<T, C, NL, P, WPB> pol;
   pol.init(red[threadIdx.x >> 5], args.out, args.ntasks, args.nl_out);
-  sweep<T, KD, C, DIFF, WPB>(args, pol, sm[threadIdx.x >> 5]);
+  sweep<T, KD, C, DIFF, WPB, EXT>(args, pol, sm[threadIdx.x >> 5]);
 }
 
 // ---------------------------------------------------------------------------
@@ -747,14 +771,14 @@ struct PdePolicy {
   __device__ void collect(long long, int, int) {}
 };
 
-template <typename T, int KD, int C, int F, bool DIFF, int WPB>
+template <typename T, int KD, int C, int F, bool DIFF, int WPB, bool EXT>
 __global__ void __launch_bounds__(WPB * 32)
 pde_fwd_kernel(const SweepArgs<T> args) {
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   auto* sm = reinterpret_cast<SweepSmem<T, KD, C>*>(dyn_smem);
   PdePolicy<T, C, F, DIFF> pol;
   pol.init(args.out);
-  sweep<T, KD, C, DIFF, WPB>(args, pol, sm[threadIdx.x >> 5]);
+  sweep<T, KD, C, DIFF, WPB, EXT>(args, pol, sm[threadIdx.x >> 5]);
 }
 
 }  // namespace ksig

@@ -163,10 +163,15 @@ class SignatureBase:
     return self
 
   def _static(self):
+    """(kind, parameter): one float for RBF / linear, the parameter tuple
+    for the other static kernels (fused into the Gram epilogue alike)."""
     sk = self.static_kernel
     if not isinstance(sk, StaticKernel) or sk.kind is None:
-      raise ValueError('static_kernel must be RBFKernel or LinearKernel')
-    return sk.kind, sk.param
+      raise ValueError('static_kernel must be one of the kernels of '
+                       'ksig_b200.static.kernels')
+    if sk.kind in (L.STATIC_RBF, L.STATIC_LINEAR):
+      return sk.kind, sk.param
+    return sk.kind, tuple(sk.params)
 
   def __call__(self, X, Y=None, diag: bool = False,
                return_on_gpu: bool = False):
@@ -211,6 +216,9 @@ class SignatureBase:
   def _K_autograd(self, Xin, Xs, gx, Ys, gy, sym):
     """Differentiable K(X, Y) / K(X) through the hand-written adjoint."""
     kind, param = self._static()
+    if kind not in (L.STATIC_RBF, L.STATIC_LINEAR):
+      raise NotImplementedError(
+          'gradients are available with the RBF and linear static kernels')
     pt = self._param_tensor()
     spec = dict(Xs=Xs, Ys=Ys, normalize=self.normalize, kind=kind,
                 param=float(param), levels_fn=self._levels,

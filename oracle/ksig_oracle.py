@@ -67,6 +67,28 @@ def static_gram(X, Y, kind='rbf', param=1.0):
     return np.exp(-d2 / max(2 * float(param) ** 2, EPS))
   if kind == 'linear':
     return float(param) * xy
+  if kind == 'poly':  # ksig/static/kernels.py:183-194, param = (degree, gamma, scale)
+    degree, gamma, scale = param
+    return scale * np.power(xy + gamma, degree)
+  xn = np.sum(np.square(X), axis=-1)
+  yn = np.sum(np.square(Y), axis=-1)
+  d2 = xn[..., :, None] + yn[..., None, :] - 2 * xy
+  if kind in ('matern12', 'matern32'):
+    # ksig/static/kernels.py:263-296 with the distance between x and y
+    # (robust_sqrt, ksig/utils.py:173-182).  The reference's euclid_dist
+    # (ksig/utils.py:186-197) takes a stray `self` argument and measures
+    # within its second set instead; this restates the intended kernel.
+    c = np.sqrt(3.) if kind == 'matern32' else 1.0
+    D = c * np.sqrt(np.maximum(d2, EPS)) / max(float(param), EPS)
+    return np.exp(-D) if kind == 'matern12' else (1. + D) * np.exp(-D)
+  if kind == 'matern52':  # ksig/static/kernels.py:299-316
+    E = 5 * d2 / max(float(param) ** 2, EPS)
+    D = np.sqrt(np.maximum(E, EPS))
+    return (1. + D + E / 3.) * np.exp(-D)
+  if kind == 'rq':  # ksig/static/kernels.py:319-343, param = (bandwidth, alpha)
+    bw, alpha = param
+    E = d2 / max(2 * alpha * bw ** 2, EPS)
+    return np.power(1 + E, -alpha)
   raise ValueError(f'unknown static kernel {kind!r}')
 
 

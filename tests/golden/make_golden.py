@@ -93,7 +93,45 @@ def _cases():
       P, Q)
   add('pde_ragged', 'pde', dict(normalize=False, static='rbf', param=0.9),
       [P[0, :5], P[1], P[2, :7]], [Q[0, :4], Q[1]], ragged=True)
+
+  # The other static kernels of ksig.static.kernels (Matern12 / 32 go
+  # through the reference's euclid_dist, which measures within the second
+  # point set, so they have no reference output to pin to).
+  add('dp_poly', 'sig', dict(n_levels=3, order=1, normalize=False,
+                              static='poly', param=[2.0, 1.0, 0.5]),
+      X1[:, :9], Y1[:, :7])
+  add('dp_poly_o2_norm', 'sig', dict(n_levels=3, order=2, normalize=True,
+                                      static='poly', param=[3.0, 0.5, 1.0]),
+      X1[:, :9], Y1[:, :7])
+  add('dp_matern52', 'sig', dict(n_levels=4, order=1, normalize=False,
+                                  static='matern52', param=0.9), X1, Y1)
+  add('dp_matern52_norm', 'sig', dict(n_levels=4, order=1, normalize=True,
+                                       static='matern52', param=0.9), X1, Y1)
+  add('dp_rq', 'sig', dict(n_levels=4, order=2, normalize=False,
+                            static='rq', param=[0.8, 1.5]), X1, Y1)
+  add('pde_matern52', 'pde', dict(normalize=False, static='matern52', param=1.1),
+      P, Q)
+  add('pde_rq_norm', 'pde', dict(normalize=True, static='rq', param=[0.7, 2.0]),
+      P, Q)
+  add('pde_poly', 'pde', dict(normalize=False, static='poly', param=[2.0, 1.0, 0.3]),
+      P[:, :6], Q[:, :5])
   return cases
+
+
+def _static(ksig, p):
+  st, v = p['static'], p['param']
+  K = ksig.static.kernels
+  if st == 'rbf':
+    return K.RBFKernel(v)
+  if st == 'linear':
+    return K.LinearKernel(v)
+  if st == 'poly':
+    return K.PolynomialKernel(degree=v[0], gamma=v[1], scale=v[2])
+  if st == 'matern52':
+    return K.Matern52Kernel(v)
+  if st == 'rq':
+    return K.RationalQuadraticKernel(bandwidth=v[0], alpha=v[1])
+  raise ValueError(st)
 
 
 def _pad_edge(seqs):
@@ -113,8 +151,7 @@ def _run_reference():
   meta = []
   for c in _cases():
     p = c['params']
-    static = (ksig.static.kernels.RBFKernel(p['param']) if p['static'] == 'rbf'
-              else ksig.static.kernels.LinearKernel(p['param']))
+    static = _static(ksig, p)
     if c['kernel'] == 'sig':
       K = ksig.kernels.SignatureKernel(
           n_levels=p['n_levels'], order=p['order'],

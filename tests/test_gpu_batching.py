@@ -137,3 +137,23 @@ def test_device_status_reaches_python():
   good = E.Seqs(X, torch.tensor([10, 7, 5], dtype=torch.int32, device='cuda'))
   E.sig_levels(good, None, Lb.PAIRS_UPPER, 3, 1, True, Lb.STATIC_RBF, 1.0)
   K.check_device_status()
+
+
+@pytest.mark.parametrize('batch_size', [None, 4, 7])
+def test_precompute_kernel_mat_matches_full_call(batch_size):
+  """Block-row precompute (the SVC caller, ksig/models/pre_base.py:88-142)
+  equals the single call, for K(X) (mirrored) and K(X, X2)."""
+  import ksig_b200 as K
+  rng = np.random.default_rng(11)
+  X = np.cumsum(rng.standard_normal((13, 20, 3)) * 0.3, axis=1)
+  X2 = np.cumsum(rng.standard_normal((6, 15, 3)) * 0.3, axis=1)
+  kern = K.SignatureKernel(n_levels=4, order=1, normalize=True,
+                           static_kernel=K.RBFKernel(0.8))
+  full = kern(X)
+  full2 = kern(X, X2)
+  got = K.precompute.precompute_kernel_mat(kern, X, None, batch_size)
+  got2 = K.precompute.precompute_kernel_mat(kern, X, X2, batch_size)
+  assert got.shape == (13, 13) and got2.shape == (13, 6)
+  np.testing.assert_allclose(got, full, rtol=1e-12, atol=1e-14)
+  np.testing.assert_allclose(got2, full2, rtol=1e-12, atol=1e-14)
+  np.testing.assert_allclose(got, got.T, rtol=0, atol=0)

@@ -19,11 +19,28 @@ DP_TOL = 1e-5
 PDE_TOL = 1e-4
 
 
+def _static(K, name, v):
+  if name == 'rbf':
+    return K.RBFKernel(v)
+  if name == 'linear':
+    return K.LinearKernel(v)
+  if name == 'poly':
+    return K.PolynomialKernel(degree=v[0], gamma=v[1], scale=v[2])
+  if name == 'matern12':
+    return K.Matern12Kernel(v)
+  if name == 'matern32':
+    return K.Matern32Kernel(v)
+  if name == 'matern52':
+    return K.Matern52Kernel(v)
+  if name == 'rq':
+    return K.RationalQuadraticKernel(bandwidth=v[0], alpha=v[1])
+  raise ValueError(name)
+
+
 def _kern(c, **over):
   import ksig_b200 as K
   p = dict(c['params'], **over)
-  static = (K.RBFKernel(p['param']) if p['static'] == 'rbf'
-            else K.LinearKernel(p['param']))
+  static = _static(K, p['static'], p['param'])
   if c['kernel'] == 'sig':
     return K.SignatureKernel(
         n_levels=p['n_levels'], order=p['order'],
@@ -253,3 +270,39 @@ def test_plain_baseline_kernel_matches_oracle(order, n_levels):
   got = got.cpu().numpy().reshape(ref.shape)
   scale = np.abs(ref).max(axis=(1, 2), keepdims=True)
   assert np.max(np.abs(got - ref) / scale) < 1e-5
+
+
+@pytest.mark.parametrize('name,param', [('matern12', 0.8), ('matern32', 1.2),
+                                        ('matern52', 0.7), ('poly', (2.0, 0.1, 0.2)),
+                                        ('rq', (0.9, 0.7))])
+@pytest.mark.parametrize('dt,tol', [(np.float64, 1e-9), (np.float32, 1e-5)])
+def test_other_static_kernels_vs_oracle(name, param, dt, tol):
+  """Every static kernel of ksig.static.kernels, fused into the Gram
+  epilogue of the DP and PDE sweeps, against the FP64 oracle (Matern12 / 32
+  with the distance between x and y; their reference outputs are not
+  usable, see oracle.ksig_oracle.static_gram)."""
+  import ksig_b200 as K
+  rng = np.random.default_rng(90)
+  X = np.cumsum(rng.standard_normal((4, 19, 3)) * 0.3, axis=1).astype(dt)
+  Y = np.cumsum(rng.standard_normal((3, 23, 3)) * 0.3, axis=1).astype(dt)
+  Xo, Yo = X.astype(np.float64), Y.astype(np.float64)
+  for normalize in (False, True):
+    sk = _static(K, name, param)
+    got = K.SignatureKernel(n_levels=4, order=2, normalize=normalize, static_kernel=sk)(X, Y)
+    ref = O.signature_kernel(Xo, Yo, n_levels=4, order=2, normalize=normalize,
+                             kind=name, param=param)
+    assert _relerr(got, ref) < tol, (name, normalize)
+    got = K.SignaturePDEKernel(normalize=normalize, static_kernel=sk, dyadic_order=1)(X)
+    ref = O.signature_pde_kernel(Xo, None, normalize=normalize, kind=name, param=param,
+                                 dyadic_order=1)
+    assert _relerr(got, ref) < max(tol, 1e-9 if dt == np.float64 else PDE_TOL), (name, normalize)
+
+
+def test_other_static_kernels_reject_gradients():
+  import ksig_b200 as K
+  X = torch.randn((2, 6, 2), dtype=torch.float64, device='cuda', requires_grad=True)
+  kern = K.SignatureKernel(n_levels=2, static_kernel=K.Matern52Kernel(1.0))
+  with pytest.raises(NotImplementedError):
+    kern(X)
+  with pytest.raises(ValueError):
+    K.RationalQuadraticKernel(bandwidth=1.0, alpha=-1.0)
