@@ -228,6 +228,29 @@ int ksig_signature_kern_pde_ex(const void* X, const int32_t* lenX, int nX,
                                int n_list, double* out, void* workspace,
                                size_t workspace_bytes, void* stream);
 
+/* Workspace (bytes) required by ksig_global_align_kern. */
+size_t ksig_global_align_kern_workspace(int nX, int LX, int nY, int LY, int d,
+                                        int dtype, int pairs_mode, int n_list);
+
+/*
+ * Global alignment kernel in log space (replaces global_align_kern_log,
+ * ksig/algorithms.py:453-559, behind GlobalAlignmentKernel._compute_kernel,
+ * ksig/kernels.py:366-409).  With M the static Gram of the pair (RBF or
+ * linear, no differencing), M' = M / (2 - M), logM = log(max(M', 1e-12)):
+ *   logK[i,j] = logM[i,j] + logsumexp(logK[i-1,j], logK[i,j-1], logK[i-1,j-1]),
+ * logK[-1,-1] = 0, -inf elsewhere on the boundary.
+ *   out_log  float64 [P]: logK at the last point pair of every pair.
+ * The normalisation of GlobalAlignmentKernel (log-space, ksig/kernels.py:
+ * 190-206) is left to the caller.
+ */
+int ksig_global_align_kern(const void* X, const int32_t* lenX, int nX,
+                           int LX, const void* Y, const int32_t* lenY, int nY,
+                           int LY, int d, int dtype, int static_kind,
+                           double static_param, int pairs_mode,
+                           const int32_t* pair_list, int n_list,
+                           double* out_log, void* workspace,
+                           size_t workspace_bytes, void* stream);
+
 /* Workspace (bytes) required by ksig_signature_kern_bwd. */
 size_t ksig_signature_kern_bwd_workspace(int nX, int LX, int nY, int LY,
                                          int d, int dtype, int n_levels,

@@ -11,7 +11,8 @@ from . import static  # noqa: F401
 from . import tuning  # noqa: F401
 from . import utils  # noqa: F401
 from .graphs import GraphedKernel  # noqa: F401
-from .kernels import Ragged, SignatureKernel, SignaturePDEKernel  # noqa: F401
+from .kernels import (GlobalAlignmentKernel, Ragged, SignatureKernel,  # noqa: F401
+                      SignaturePDEKernel)
 from .static.kernels import (LinearKernel, Matern12Kernel, Matern32Kernel,  # noqa: F401
                              Matern52Kernel, PolynomialKernel, RationalQuadraticKernel,
                              RBFKernel)

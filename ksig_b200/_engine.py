@@ -216,6 +216,33 @@ def sig_levels_bwd_plain(X, Y, mode, n_levels, order, kind, param, grad_levels,
   return dX, dpar
 
 
+def ga_values(X, Y, mode, kind, param, pair_list=None):
+  """Log global-alignment kernel per pair ``[P]`` (float64)."""
+  lib = L.lib()
+  Yv = X if Y is None else Y
+  dt = _dtype_code(X.data)
+  if Y is not None and Y.data.dtype != X.data.dtype:
+    raise ValueError('X and Y must share a dtype')
+  if Y is not None and Y.d != X.d:
+    raise ValueError('X and Y must have the same number of features')
+  n_list = 0 if pair_list is None else pair_list.shape[0]
+  P = num_pairs(mode, X.n, Yv.n, n_list)
+  out = torch.empty((max(P, 0),), dtype=torch.float64, device=X.data.device)
+  ws_bytes = lib.ksig_global_align_kern_workspace(
+      X.n, X.L, Yv.n, Yv.L, X.d, dt, mode, n_list)
+  if ws_bytes == 0:
+    L.check(L.ERR_UNSUPPORTED if 'no compiled' in L.last_error()
+            else L.ERR_INVALID)
+  ws = _workspace(ws_bytes, X.data.device)
+  rc = lib.ksig_global_align_kern(
+      _ptr(X.data), _ptr(X.lengths), X.n, X.L, _ptr(Yv.data),
+      _ptr(Yv.lengths), Yv.n, Yv.L, X.d, dt, kind, float(param), mode,
+      _ptr(pair_list), n_list, _ptr(out), _ptr(ws), ws_bytes, _stream())
+  L.check(rc)
+  _fold_status(ws)
+  return out
+
+
 def pde_values(X, Y, mode, dyadic_order, difference, kind, param,
                pair_list=None):
   """Signature-PDE kernel per pair ``[P]`` (float64)."""

@@ -80,6 +80,9 @@ _SIGNATURES = {
     'ksig_signature_kern_pde_ex': (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _I,
                                         _I, _I, _P, _I, _I, _I, _P, _I, _P,
                                         _P, _SZ, _P]),
+    'ksig_global_align_kern_workspace': (_SZ, [_I] * 8),
+    'ksig_global_align_kern': (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _I, _I,
+                                    _I, _D, _I, _P, _I, _P, _P, _SZ, _P]),
     'ksig_launch_count': (ctypes.c_ulonglong, []),
     'ksig_profile_enable': (None, [_I]),
     'ksig_profile_read': (_I, [ctypes.POINTER(ctypes.c_double),

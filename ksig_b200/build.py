@@ -83,6 +83,11 @@ def instances():
         add(('dpx', dt, kd, c, nl, p, 1))
     for f, kd in itertools.product([1, 2, 4, 8], KD_FEW):
       add(('pdex', dt, kd, c, 0, f, 1))
+  # Global alignment kernel (no differencing).
+  for kd, c in itertools.product(KD_ALL, [2, 4, 8]):
+    add(('ga', 'f32', kd, c, 0, 1, 0))
+  for kd in KD_MID:
+    add(('ga', 'f64', kd, 2, 0, 1, 0))
   # PDE backward (row-side gradients).
   for f, kd, c in itertools.product([1, 2, 4, 8], KD_MID, [2, 4, 8]):
     if c * f <= 16:  # the adjoint keeps three C*F-wide rows in registers
@@ -106,6 +111,7 @@ OPS = {
     'pde': ('OP_PDE_FWD', 'pde_fwd_kernel<{T}, {kd}, {c}, {p}, {diff}, {wpb}, false>'),
     'dpx': ('OP_DP_FWD_EXT', 'dp_fwd_kernel<{T}, {kd}, {c}, {nl}, {p}, {diff}, {wpb}, true>'),
     'pdex': ('OP_PDE_FWD_EXT', 'pde_fwd_kernel<{T}, {kd}, {c}, {p}, {diff}, {wpb}, true>'),
+    'ga': ('OP_GA_FWD', 'ga_fwd_kernel<{T}, {kd}, {c}, {wpb}>'),
     'dpb': ('OP_DP_BWD', 'dp_bwd_kernel<{T}, {kd}, {c}, {nl}, {p}, {wpb}>'),
     'pdeb': ('OP_PDE_BWD', 'pde_bwd_kernel<{T}, {kd}, {c}, {p}, {wpb}>'),
 }

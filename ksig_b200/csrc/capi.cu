@@ -300,9 +300,12 @@ int want_cols(int ly_cells, int cap, int op) {
   return cap;
 }
 
-int plan_fwd(bool pde, int nX, int LX, int nY, int LY, int d, int dtype, int n_levels,
+// family: 0 DP, 1 PDE (order_or_dyadic = dyadic order), 2 global alignment
+// (no differencing; order_or_dyadic unused).
+int plan_fwd(int family, int nX, int LX, int nY, int LY, int d, int dtype, int n_levels,
              int order_or_dyadic, int difference, int pairs_mode, int n_list,
              FwdPlan& pl, bool allow_order = true, bool ext = false) {
+  const bool pde = family == 1, ga = family == 2;
   if (dtype != KSIG_DTYPE_F32 && dtype != KSIG_DTYPE_F64)
     return fail(KSIG_ERR_INVALID, "dtype must be KSIG_DTYPE_F32 or KSIG_DTYPE_F64");
   if (nX <= 0 || LX <= 0 || d <= 0) return fail(KSIG_ERR_INVALID, "empty X (n=%d, L=%d, d=%d)", nX, LX, d);
@@ -316,7 +319,10 @@ int plan_fwd(bool pde, int nX, int LX, int nY, int LY, int d, int dtype, int n_l
   pl.diff = difference ? 1 : 0;
   pl.ntasks = np;
   int need_nl = 0, p = 0;
-  if (pde) {
+  if (ga) {
+    pl.diff = 0;
+    p = 1;
+  } else if (pde) {
     if (order_or_dyadic < 0 || order_or_dyadic > 3)
       return fail(KSIG_ERR_UNSUPPORTED, "dyadic_order %d not in [0, 3]", order_or_dyadic);
     p = 1 << order_or_dyadic;
@@ -330,13 +336,15 @@ int plan_fwd(bool pde, int nX, int LX, int nY, int LY, int d, int dtype, int n_l
   }
   const int ly_cells = pl.diff ? LY - 1 : LY;
   const int lx_cells = pl.diff ? LX - 1 : LX;
-  const int op = ext ? (pde ? OP_PDE_FWD_EXT : OP_DP_FWD_EXT) : (pde ? OP_PDE_FWD : OP_DP_FWD);
+  const int op = ga ? OP_GA_FWD
+                   : ext ? (pde ? OP_PDE_FWD_EXT : OP_DP_FWD_EXT) : (pde ? OP_PDE_FWD : OP_DP_FWD);
   const int want = want_cols(ly_cells, 8, op);
   const KernelEntry* k = find_kernel(op, pl.f64, d, want, need_nl, p, pl.diff);
   if (!k)
     return fail(KSIG_ERR_UNSUPPORTED,
                 "no compiled %s kernel for dtype=%s d=%d n_levels=%d order/F=%d difference=%d%s",
-                pde ? "PDE" : "DP", pl.f64 ? "f64" : "f32", d, n_levels, p, pl.diff,
+                ga ? "global-alignment" : pde ? "PDE" : "DP", pl.f64 ? "f64" : "f32", d, n_levels,
+                p, pl.diff,
                 ext ? " (polynomial / Matern / rational quadratic static kernel)" : "");
   pl.k = k;
   pl.kd = k->kd;
@@ -349,7 +357,9 @@ int plan_fwd(bool pde, int nX, int LX, int nY, int LY, int d, int dtype, int n_l
   pl.rs = round_up(pl.kd + 1, (int)(16 / es));
   const int strip = pl.diff ? 32 * pl.c - 1 : 32 * pl.c;
   pl.multi = ly_cells > strip ? 1 : 0;
-  if (pde) {
+  if (ga) {
+    pl.nx_exchange = 1;
+  } else if (pde) {
     pl.nx_exchange = 2 * p;
   } else {
     int nh = 0;
@@ -883,7 +893,7 @@ int check_common(const void* X, const void* Y, int pairs_mode, const int32_t* li
   return KSIG_OK;
 }
 
-int fwd_entry(bool pde, const void* X, const int32_t* lenX, int nX, int LX, const void* Y,
+int fwd_entry(int family, const void* X, const int32_t* lenX, int nX, int LX, const void* Y,
               const int32_t* lenY, int nY, int LY, int d, int dtype, int static_kind,
               double static_param, int n_levels, int order_or_dyadic, int difference,
               int pairs_mode, const int32_t* list, int n_list, double* out, void* ws,
@@ -904,8 +914,8 @@ int fwd_entry(bool pde, const void* X, const int32_t* lenX, int nX, int LX, cons
   if (!out) return fail(KSIG_ERR_INVALID, "output is NULL");
   FwdPlan pl;
   const bool ext = static_kind != KSIG_STATIC_RBF && static_kind != KSIG_STATIC_LINEAR;
-  rc = plan_fwd(pde, nX, LX, nY, LY, d, dtype, n_levels, order_or_dyadic, difference, pairs_mode,
-                n_list, pl, allow_order, ext);
+  rc = plan_fwd(family, nX, LX, nY, LY, d, dtype, n_levels, order_or_dyadic, difference,
+                pairs_mode, n_list, pl, allow_order, ext);
   if (rc) return rc;
   if (!ws || ws_bytes < pl.total)
     return fail(KSIG_ERR_WORKSPACE, "workspace of %zu bytes is smaller than the %zu required",
@@ -1073,6 +1083,23 @@ int ksig_signature_kern_pde_ex(const void* X, const int32_t* lenX, int nX, int L
   return fwd_entry(true, X, lenX, nX, LX, Y, lenY, nY, LY, d, dtype, static_kind,
                    static_params[0], 0, dyadic_order, difference, pairs_mode, pair_list, n_list,
                    out, workspace, workspace_bytes, stream, true, static_params);
+}
+
+size_t ksig_global_align_kern_workspace(int nX, int LX, int nY, int LY, int d, int dtype,
+                                        int pairs_mode, int n_list) {
+  FwdPlan pl;
+  if (plan_fwd(2, nX, LX, nY, LY, d, dtype, 0, 0, 0, pairs_mode, n_list, pl)) return 0;
+  return pl.total;
+}
+
+int ksig_global_align_kern(const void* X, const int32_t* lenX, int nX, int LX, const void* Y,
+                           const int32_t* lenY, int nY, int LY, int d, int dtype,
+                           int static_kind, double static_param, int pairs_mode,
+                           const int32_t* pair_list, int n_list, double* out_log,
+                           void* workspace, size_t workspace_bytes, void* stream) {
+  return fwd_entry(2, X, lenX, nX, LX, Y, lenY, nY, LY, d, dtype, static_kind, static_param, 0,
+                   0, 0, pairs_mode, pair_list, n_list, out_log, workspace, workspace_bytes,
+                   stream);
 }
 
 int ksig_signature_kern_static(const void* X, const int32_t* lenX, int nX, int LX,

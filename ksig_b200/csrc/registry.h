@@ -13,6 +13,7 @@ enum KernelOp : int {
   OP_PDE_BWD = 3,  // PdeBwdArgs<T>         pde_bwd_kernel
   OP_DP_FWD_EXT = 4,   // dp_fwd_kernel, EXT: the other static kernels
   OP_PDE_FWD_EXT = 5,  // pde_fwd_kernel, EXT
+  OP_GA_FWD = 6,       // SweepArgs<T>      ga_fwd_kernel (global alignment)
 };
 
 struct KernelEntry {

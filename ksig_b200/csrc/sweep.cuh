@@ -781,4 +781,97 @@ pde_fwd_kernel(const SweepArgs<T> args) {
   sweep<T, KD, C, DIFF, WPB, EXT>(args, pol, sm[threadIdx.x >> 5]);
 }
 
+// ---------------------------------------------------------------------------
+// Global alignment kernel (ksig/algorithms.py:453-559), no differencing: the
+// "cells" are the grid points, Z carries the static-kernel values M.  In log
+// space, with M' = M / (2 - M) and logM = log(max(M', 1e-12)),
+//   logK[i,j] = logM[i,j] + LSE(logK[i-1,j], logK[i,j-1], logK[i-1,j-1]),
+// logK[-1,-1] = 0 and -inf elsewhere on the boundary; the result is logK at
+// the last point pair.  The neighbour pattern is the PDE's at F = 1: the
+// left value and the corner come from lane l-1, the upper row stays in the
+// lane's registers.
+// ---------------------------------------------------------------------------
+
+template <typename T>
+__device__ __forceinline__ T ga_logm(T m) {
+  const T mp = m / (T(2) - m);
+  return log(fmax(mp, T(1e-12)));
+}
+
+template <typename T>
+__device__ __forceinline__ T lse3(T a, T b, T c) {
+  const T m = fmax(a, fmax(b, c));
+  if (!(m > -INFINITY)) return m;  // all three -inf (or a NaN input)
+  return m + log(exp(a - m) + exp(b - m) + exp(c - m));
+}
+
+template <typename T, int C>
+struct GaPolicy {
+  static constexpr int NX = 1;
+  static constexpr bool kUnroll2 = false;
+  static constexpr int STRIP = 32 * C;
+  T X[NX];
+  T Kr[C];       // logK of the row above, the lane's columns
+  T kcorner;     // logK at the lane's left boundary on the row above
+  double* out;
+  int tgt_s, tgt_lane, tgt_c, tgt_r;
+
+  __device__ void init(double* out_) {
+    out = out_;
+    tgt_s = -1; tgt_lane = -1; tgt_c = 0; tgt_r = -1;
+    X[0] = T(-INFINITY);
+  }
+  __device__ void begin_item() {
+#pragma unroll
+    for (int c = 0; c < C; ++c) Kr[c] = T(-INFINITY);
+    kcorner = T(-INFINITY);
+  }
+  __device__ void begin_task(const ItemInfo& it, int lane) {
+    if (lane == 0) kcorner = T(0);  // logK[-1, -1] = log 1
+    tgt_r = it.Lx - 1;
+    const int col = it.Ly - 1;
+    tgt_s = col / STRIP;
+    const int rem = col - tgt_s * STRIP;
+    tgt_lane = rem / C;
+    tgt_c = rem - tgt_lane * C;
+  }
+  __device__ void left_boundary(T (&Xin)[NX]) { Xin[0] = T(-INFINITY); }
+
+  __device__ void row(const T (&Z)[C], const T (&Xin)[NX], bool, bool valid, int r,
+                      const ItemInfo& it, int lane) {
+    if (!valid) return;
+    T klo = kcorner;
+    T kln = Xin[0];
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      const T up = Kr[c];
+      const T v = ga_logm(Z[c]) + lse3(up, kln, klo);
+      klo = up;
+      kln = v;
+      Kr[c] = v;
+    }
+    X[0] = kln;
+    kcorner = Xin[0];
+    if (r == tgt_r && it.s == tgt_s && lane == tgt_lane) {
+      T captured = T(0);
+#pragma unroll
+      for (int c = 0; c < C; ++c) captured = (c == tgt_c) ? Kr[c] : captured;
+      out[it.task] = (double)captured;
+    }
+  }
+  __device__ void end_item() {}
+  __device__ void end_task(long long, int, int) {}
+  __device__ void collect(long long, int, int) {}
+};
+
+template <typename T, int KD, int C, int WPB>
+__global__ void __launch_bounds__(WPB * 32)
+ga_fwd_kernel(const SweepArgs<T> args) {
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  auto* sm = reinterpret_cast<SweepSmem<T, KD, C>*>(dyn_smem);
+  GaPolicy<T, C> pol;
+  pol.init(args.out);
+  sweep<T, KD, C, false, WPB, false>(args, pol, sm[threadIdx.x >> 5]);
+}
+
 }  // namespace ksig

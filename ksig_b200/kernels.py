@@ -308,3 +308,66 @@ class SignaturePDEKernel(SignatureKernel):
     kind, param = self._static()
     return E.pde_values_bwd(Xs, Ys, mode, self.dyadic_order, kind, param,
                             grad_levels[0], want_dparam=want_dparam)
+
+
+class GlobalAlignmentKernel(SignatureBase):
+  """Global alignment kernel (ksig/kernels.py:366-409), always normalised.
+
+  ``K(x, y) = exp(logGA(x, y) - (logGA(x, x) + logGA(y, y)) / 2)`` with the
+  log-space alignment recursion of ksig/algorithms.py:453-559 run by the
+  persistent skewed sweep (``ksig_global_align_kern``); the normalisation
+  follows the log-space branch of ksig/kernels.py:190-206 and
+  ``K(X, diag=True)`` returns ones.  Static kernels: RBF and linear.
+  """
+
+  def __init__(self, n_features: Optional[int] = None,
+               static_kernel: Optional[StaticKernel] = None):
+    self.n_features = (utils.check_positive_value(n_features, 'n_features')
+                       if n_features is not None else None)
+    self.static_kernel = static_kernel or static_mod.kernels.RBFKernel()
+
+  @property
+  def normalize(self):
+    return True
+
+  @property
+  def is_log_space(self):
+    return True
+
+  def _static(self):
+    kind, param = super()._static()
+    if kind not in (L.STATIC_RBF, L.STATIC_LINEAR):
+      raise ValueError('GlobalAlignmentKernel supports the RBF and linear '
+                       'static kernels')
+    return kind, param
+
+  def __call__(self, X, Y=None, diag: bool = False,
+               return_on_gpu: bool = False):
+    if not torch.cuda.is_available():
+      raise RuntimeError('ksig_b200 needs a CUDA device (no CPU fallback)')
+    Xs, _, _ = _to_seqs(X, self.n_features)
+    if diag:
+      K = torch.ones((Xs.n,), dtype=torch.float64, device=Xs.data.device)
+    else:
+      kind, param = self._static()
+      if Y is None:
+        up = E.ga_values(Xs, None, L.PAIRS_UPPER, kind, param)
+        n = Xs.n
+        iu = torch.triu_indices(n, n, device=up.device)
+        lk = torch.empty((n, n), dtype=torch.float64, device=up.device)
+        lk[iu[0], iu[1]] = up
+        lk[iu[1], iu[0]] = up
+        d = torch.diagonal(lk)
+        lk = lk - 0.5 * (d[:, None] + d[None, :])
+      else:
+        Ys, _, _ = _to_seqs(Y, self.n_features)
+        lk = E.ga_values(Xs, Ys, L.PAIRS_FULL, kind, param).reshape(Xs.n, Ys.n)
+        dx = E.ga_values(Xs, None, L.PAIRS_DIAG, kind, param)
+        dy = E.ga_values(Ys, None, L.PAIRS_DIAG, kind, param)
+        lk = lk - 0.5 * (dx[:, None] + dy[None, :])
+      K = torch.exp(lk).to(Xs.data.dtype)
+    if return_on_gpu:
+      return K
+    out = K.detach().cpu().numpy()
+    E.check_device_status()
+    return out

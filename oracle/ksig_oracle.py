@@ -42,7 +42,7 @@ __all__ = [
     'EPS', 'static_gram', 'second_difference', 'multi_cumsum_exclusive',
     'sig_levels_first_order', 'sig_levels_higher_order', 'sig_levels',
     'sig_pde', 'signature_kernel', 'signature_pde_kernel', 'as_seq_list',
-    'normalize_levels',
+    'normalize_levels', 'ga_log', 'global_align_kernel',
 ]
 
 
@@ -313,3 +313,46 @@ def signature_pde_kernel(X, Y=None, diag=False, difference=True,
   """
   fn = lambda Z: sig_pde(Z, dyadic_order)  # noqa: E731
   return _front(X, Y, diag, normalize, fn, kind, param, difference)
+
+
+# ----------------------------------------------------------------------------
+# Global alignment kernel.
+# ----------------------------------------------------------------------------
+
+def ga_log(M):
+  """Log global-alignment value of one pair from its static Gram ``M
+  [lx, ly]`` (ksig/algorithms.py:513-559 and the antidiagonal kernel
+  :453-510): ``M' = M / (2 - M)``, ``logM = log(max(M', 1e-12))``,
+  ``logK[i,j] = logM[i,j] + logsumexp(logK[i-1,j], logK[i,j-1],
+  logK[i-1,j-1])`` with ``logK[-1,-1] = 0`` and ``-inf`` elsewhere on the
+  boundary; returns ``logK[lx-1, ly-1]``."""
+  M = np.asarray(M, dtype=np.float64)
+  logM = np.log(np.maximum(M / (2. - M), EPS))
+  lx, ly = logM.shape
+  K = np.full((lx + 1, ly + 1), -np.inf)
+  K[0, 0] = 0.0
+  for i in range(1, lx + 1):
+    for j in range(1, ly + 1):
+      a, b, c = K[i - 1, j], K[i, j - 1], K[i - 1, j - 1]
+      m = max(a, b, c)
+      K[i, j] = logM[i - 1, j - 1] + (
+          m + np.log(np.exp(a - m) + np.exp(b - m) + np.exp(c - m)) if m > -np.inf else -np.inf)
+  return K[lx, ly]
+
+
+def global_align_kernel(X, Y=None, diag=False, kind='rbf', param=1.0):
+  """FP64 ``GlobalAlignmentKernel(...)(X, Y, diag)`` (ksig/kernels.py:366-409
+  with the log-space normalisation of :190-206; diag returns ones)."""
+  Xs = as_seq_list(X)
+  if diag:
+    return np.ones((len(Xs),))
+  Ys = Xs if Y is None else as_seq_list(Y)
+  lk = np.array([[ga_log(static_gram(x, y, kind, param)) for y in Ys] for x in Xs])
+  if Y is None:
+    d = np.diagonal(lk)
+    lk = lk - 0.5 * (d[:, None] + d[None, :])
+  else:
+    dx = np.array([ga_log(static_gram(x, x, kind, param)) for x in Xs])
+    dy = np.array([ga_log(static_gram(y, y, kind, param)) for y in Ys])
+    lk = lk - 0.5 * (dx[:, None] + dy[None, :])
+  return np.exp(lk)

@@ -115,6 +115,13 @@ def _cases():
       P, Q)
   add('pde_poly', 'pde', dict(normalize=False, static='poly', param=[2.0, 1.0, 0.3]),
       P[:, :6], Q[:, :5])
+
+  # Global alignment kernel (ksig/kernels.py:366-409).
+  rng = np.random.default_rng(14)
+  G1 = np.cumsum(rng.standard_normal((4, 11, 3)) * 0.4, axis=1)
+  G2 = np.cumsum(rng.standard_normal((3, 8, 3)) * 0.4, axis=1)
+  add('ga_rbf', 'ga', dict(normalize=True, static='rbf', param=1.2), G1, G2)
+  add('ga_linear', 'ga', dict(normalize=True, static='linear', param=0.4), G1, G2)
   return cases
 
 
@@ -157,10 +164,12 @@ def _run_reference():
           n_levels=p['n_levels'], order=p['order'],
           difference=p.get('difference', True), normalize=p['normalize'],
           static_kernel=static)
-    else:
+    elif c['kernel'] == 'pde':
       K = ksig.kernels.SignaturePDEKernel(
           difference=p.get('difference', True), normalize=p['normalize'],
           static_kernel=static)
+    else:
+      K = ksig.kernels.GlobalAlignmentKernel(static_kernel=static)
     X, Y = c['X'], c['Y']
     name = c['name']
     if c['ragged']:

@@ -46,6 +46,8 @@ def _kern(c, **over):
         n_levels=p['n_levels'], order=p['order'],
         difference=p.get('difference', True), normalize=p['normalize'],
         static_kernel=static)
+  if c['kernel'] == 'ga':
+    return K.GlobalAlignmentKernel(static_kernel=static)
   return K.SignaturePDEKernel(difference=p.get('difference', True),
                               normalize=p['normalize'], static_kernel=static,
                               dyadic_order=p.get('dyadic_order', 0))
@@ -58,6 +60,8 @@ def _oracle(c, X, Y=None, diag=False, **over):
         X, Y, diag=diag, n_levels=p['n_levels'], order=p['order'],
         difference=p.get('difference', True), normalize=p['normalize'],
         kind=p['static'], param=p['param'])
+  if c['kernel'] == 'ga':
+    return O.global_align_kernel(X, Y, diag=diag, kind=p['static'], param=p['param'])
   return O.signature_pde_kernel(
       X, Y, diag=diag, difference=p.get('difference', True),
       normalize=p['normalize'], kind=p['static'], param=p['param'],
@@ -95,6 +99,18 @@ def test_golden_fp32(c):
   tol = DP_TOL if c['kernel'] == 'sig' else PDE_TOL
   out = k(X32, Y32)
   assert out.dtype == np.float32
+  if c['kernel'] == 'ga':
+    # Alignment values span hundreds of decades; compare the entries an
+    # FP32 output can represent (the rest underflow to 0 as they would in
+    # the reference run in FP32).
+    def check(a, b):
+      m = b > 1e-30
+      assert np.all(a[~m] < 1e-28)
+      assert _relerr(a[m], b[m]) < tol
+    check(out, _oracle(c, X64, Y64))
+    check(k(X32), _oracle(c, X64))
+    assert _relerr(k(X32, diag=True), _oracle(c, X64, diag=True)) < tol
+    return
   assert _relerr(out, _oracle(c, X64, Y64)) < tol
   assert _relerr(k(X32), _oracle(c, X64)) < tol
   assert _relerr(k(X32, diag=True), _oracle(c, X64, diag=True)) < tol
@@ -306,3 +322,22 @@ def test_other_static_kernels_reject_gradients():
     kern(X)
   with pytest.raises(ValueError):
     K.RationalQuadraticKernel(bandwidth=1.0, alpha=-1.0)
+
+
+def test_global_alignment_ragged_multi_strip():
+  """Global alignment on ragged batches whose column sequences span several
+  strips, FP64 against the oracle and FP32 within the PDE tolerance."""
+  import ksig_b200 as K
+  rng = np.random.default_rng(95)
+  xs = [np.cumsum(rng.standard_normal((n, 2)) * 0.2, 0) for n in (40, 290, 7)]
+  ys = [np.cumsum(rng.standard_normal((n, 2)) * 0.2, 0) for n in (300, 12)]
+  ref = O.global_align_kernel(xs, ys, kind='rbf', param=0.9)
+  refx = O.global_align_kernel(xs, None, kind='rbf', param=0.9)
+  kern = K.GlobalAlignmentKernel(static_kernel=K.RBFKernel(0.9))
+  assert _relerr(kern(xs, ys), ref) < 1e-9
+  assert _relerr(kern(xs), refx) < 1e-9
+  got = kern([x.astype(np.float32) for x in xs], [y.astype(np.float32) for y in ys])
+  ref32 = O.global_align_kernel([x.astype(np.float32).astype(np.float64) for x in xs],
+                                [y.astype(np.float32).astype(np.float64) for y in ys],
+                                kind='rbf', param=0.9)
+  assert _relerr(got, ref32) < PDE_TOL

@@ -15,6 +15,8 @@ def _oracle(c, X, Y=None, diag=False):
         X, Y, diag=diag, n_levels=p['n_levels'], order=p['order'],
         difference=p.get('difference', True), normalize=p['normalize'],
         kind=p['static'], param=p['param'])
+  if c['kernel'] == 'ga':
+    return O.global_align_kernel(X, Y, diag=diag, kind=p['static'], param=p['param'])
   return O.signature_pde_kernel(
       X, Y, diag=diag, difference=p.get('difference', True),
       normalize=p['normalize'], kind=p['static'], param=p['param'])
