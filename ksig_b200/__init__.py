@@ -7,6 +7,7 @@ Importing the package does not touch the GPU; the CUDA library
 from . import graphs  # noqa: F401
 from . import kernels  # noqa: F401
 from . import precompute  # noqa: F401
+from . import preprocessing  # noqa: F401
 from . import static  # noqa: F401
 from . import tuning  # noqa: F401
 from . import utils  # noqa: F401

@@ -7,10 +7,11 @@ checked out at ``--ref`` (default ``/root/reference``)::
 
 The reference needs CuPy and a CUDA device.  Neither is needed here: the
 NumPy-backed ``cupy`` stand-in in ``tests/_refshim`` takes CuPy's place and
-Numba's CUDA simulator (``NUMBA_ENABLE_CUDASIM=1``) runs the Numba PDE kernel
-of ksig/algorithms.py:344-399 unchanged.  Every case stores its inputs, its
-parameters and the reference's outputs in ``golden.npz``; the tests read only
-that file, never the reference.
+Numba's CUDA simulator (``NUMBA_ENABLE_CUDASIM=1``) runs the Numba PDE and
+global-alignment kernels of ksig/algorithms.py unchanged.  Every case stores
+its inputs, its parameters and the reference's outputs in ``golden.npz``
+(kernels) and ``preprocessing.npz`` (ksig/preprocessing.py); the tests read
+only those files, never the reference.
 """
 
 import argparse
@@ -194,6 +195,36 @@ def _run_reference():
   print('wrote', len(meta), 'cases')
 
 
+def _run_preprocessing():
+  """Reference outputs of ksig/preprocessing.py (writes preprocessing.npz)."""
+  import numpy as np
+  import ksig
+  P = ksig.preprocessing
+  rng = np.random.default_rng(21)
+  out = {}
+  seqs = [np.cumsum(rng.standard_normal((n, 2)), 0) for n in (5, 9, 7)]
+  seqs[1][3, 1] = np.nan
+  for i, s in enumerate(seqs):
+    out[f'tab_ragged/in{i}'] = s
+  out['tab_ragged/out'] = P.SequenceTabulator().fit(seqs).transform(seqs)
+  eq = rng.standard_normal((3, 8, 2))
+  out['tab_max6/in'] = eq
+  out['tab_max6/out'] = P.SequenceTabulator(max_len=6).fit(eq).transform(eq.copy())
+  out['tab_same/in'] = eq
+  out['tab_same/out'] = P.SequenceTabulator().fit(eq).transform(eq.copy())
+  X = np.abs(rng.standard_normal((3, 10, 2))) + 0.5
+  out['aug_default/in'] = X
+  out['aug_default/out'] = P.SequenceAugmentor().fit(X).transform(X.copy())
+  A = P.SequenceAugmentor(lead_lag=False, max_time=2.5, basepoint=False,
+                          normalize=False)
+  out['aug_time/in'] = X
+  out['aug_time/out'] = A.fit(X).transform(X.copy())
+  out['aug_maxlen/in'] = X
+  out['aug_maxlen/out'] = P.SequenceAugmentor(max_len=15).fit(X).transform(X.copy())
+  np.savez_compressed(os.path.join(HERE, 'preprocessing.npz'), **out)
+  print('wrote preprocessing fixtures')
+
+
 def main():
   ap = argparse.ArgumentParser()
   ap.add_argument('--ref', default='/root/reference')
@@ -201,6 +232,7 @@ def main():
   a = ap.parse_args()
   if a._child:
     _run_reference()
+    _run_preprocessing()
     return
   env = dict(os.environ)
   env['PYTHONPATH'] = os.pathsep.join([SHIM, a.ref])
