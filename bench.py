@@ -154,6 +154,25 @@ class ClockSampler:
 # GPU arm.
 # ---------------------------------------------------------------------------
 
+def _other_bounds(traffic, k_ms):
+  """HBM and tensor-core fractions of the sweep against MEASURED_PEAKS.json
+  (driver-measured copy bandwidth and bf16 GEMM rate of this pool)."""
+  path = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+  try:
+    with open(path) as f:
+      pk = json.load(f)
+  except (OSError, ValueError):
+    return None
+  out = {'tensor': {'achieved': 0.0, 'peak': pk.get('bf16_tflops'), 'unit': 'TFLOP/s',
+                    'frac': 0.0, 'note': 'no tensor-core work (d <= 16 dot products)'}}
+  if traffic and k_ms:
+    gbs = traffic / (k_ms * 1e-3) / 1e9
+    out['hbm'] = {'achieved': gbs, 'peak': pk.get('hbm_gbs'), 'unit': 'GB/s',
+                  'frac': gbs / pk['hbm_gbs'] if pk.get('hbm_gbs') else None,
+                  'source': 'MEASURED_PEAKS.json'}
+  return out
+
+
 def run_ours(args, rank, world, dist):
   import torch
 
@@ -334,7 +353,10 @@ def run_ours(args, rank, world, dist):
                      'kernel': 'dp_fwd_kernel (512x512 pair sweep)',
                      'kernel_ms': k_ms,
                      'peak_source': 'measured live: FP32 FMA-chain probe '
-                                    '(ksig_fp32_peak) on this GPU'},
+                                    '(ksig_fp32_peak) on this GPU',
+                     # The other two ceilings, for context: the kernel moves
+                     # ~10 MB of DRAM per launch and issues no tensor work.
+                     'other_bounds': _other_bounds(traffic, k_ms)},
         'e2e': {'value': entries / (e_step * 1e-3), 'unit': UNIT,
                 'ms_per_step': e_step,
                 'h2d_bytes_per_step': int(X.nbytes + Y.nbytes),
