@@ -94,6 +94,15 @@ def instances():
       add(('pdeb', 'f32', kd, c, 0, f, 1))
   for f, kd in itertools.product([1, 2, 4, 8], KD_FEW):
     add(('pdeb', 'f64', kd, 2, 0, f, 1))
+  # Deep truncations (n_levels 10 and 12, order 1): the narrower tiles only,
+  # since the per-level column sums grow the register state.
+  for nl, kd, c in itertools.product([10, 12], KD_MID, [2, 4]):
+    add(('dp', 'f32', kd, c, nl, 1, 1))
+  for nl, kd in itertools.product([10, 12], KD_FEW):
+    add(('dp', 'f64', kd, 2, nl, 1, 1))
+    add(('dpb', 'f64', kd, 2, nl, 1, 1))
+  for nl, kd, c in itertools.product([10, 12], KD_MID, [2, 4]):
+    add(('dpb', 'f32', kd, c, nl, 1, 1))
   # DP backward (row-side gradients).
   for dt, cs, kds in (('f32', [2, 4, 7], KD_MID), ('f64', [2], KD_FEW)):
     for nl, kd, c in itertools.product(NL_ALL, kds, cs):

@@ -341,3 +341,20 @@ def test_global_alignment_ragged_multi_strip():
                                 [y.astype(np.float32).astype(np.float64) for y in ys],
                                 kind='rbf', param=0.9)
   assert _relerr(got, ref32) < PDE_TOL
+
+
+@pytest.mark.parametrize('n_levels', [7, 10, 12])
+def test_deep_truncation_levels(n_levels):
+  """n_levels beyond the common range (the kernels for 10 and 12 levels;
+  7 runs the 8-level kernel and drops the top level)."""
+  import ksig_b200 as K
+  rng = np.random.default_rng(97)
+  X = np.cumsum(rng.standard_normal((3, 30, 3)) * 0.3, axis=1)
+  Y = np.cumsum(rng.standard_normal((2, 25, 3)) * 0.3, axis=1)
+  ref = O.signature_kernel(X, Y, n_levels=n_levels, normalize=True, param=0.7)
+  kern = K.SignatureKernel(n_levels=n_levels, static_kernel=K.RBFKernel(0.7))
+  assert _relerr(kern(X, Y), ref) < 1e-9
+  assert _relerr(kern(X.astype(np.float32), Y.astype(np.float32)),
+                 O.signature_kernel(X.astype(np.float32).astype(np.float64),
+                                    Y.astype(np.float32).astype(np.float64),
+                                    n_levels=n_levels, normalize=True, param=0.7)) < DP_TOL

@@ -162,3 +162,15 @@ def test_plain_bwd_baseline_matches_fused(dt, tol, order, n_levels, kind):
   dXp, dpp = E.sig_levels_bwd_plain(Xs, Ys, 0, n_levels, order, kind, param, gl)
   assert _relerr(dXp, dXf) < tol
   assert abs(dpp.item() - dpf.item()) <= tol * max(1.0, abs(dpf.item()))
+
+
+@pytest.mark.parametrize('dt,tol', [(torch.float64, 1e-8), (torch.float32, 1e-4)])
+def test_dp_grad_deep_truncation(dt, tol):
+  rng = np.random.default_rng(98)
+  X = _walks(rng, 2, 14, 2)
+  Y = _walks(rng, 2, 11, 2)
+  _run(lambda K, b: K.SignatureKernel(n_levels=10, order=1, normalize=True,
+                                      static_kernel=K.RBFKernel(b)),
+       lambda x, y, b: OT.signature_kernel(x, y, n_levels=10, order=1,
+                                           normalize=True, param=b),
+       X, Y, 0.9, dt, tol)
