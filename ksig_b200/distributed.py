@@ -17,8 +17,9 @@ exchange step the adjoint has.  If every rank evaluates the same loss on
 the gathered matrix, scale that loss by 1 / world_size.
 """
 
-from typing import Callable, Optional, Tuple
+from typing import Callable, Optional, Sequence, Tuple
 
+import numpy as np
 import torch
 import torch.distributed as dist
 
@@ -78,3 +79,75 @@ def allreduce_grads(tensors, group: Optional['dist.ProcessGroup'] = None):
   for t in tensors:
     if t is not None and t.grad is not None:
       dist.all_reduce(t.grad, op=dist.ReduceOp.SUM, group=group)
+
+
+def upper_pairs(n: int) -> np.ndarray:
+  """The upper triangle of an n x n Gram (a <= b), row-major: the order of
+  the library's KSIG_PAIRS_UPPER enumeration.  int32 [n(n+1)/2, 2]."""
+  a, b = np.triu_indices(n)
+  return np.stack([a, b], axis=1).astype(np.int32)
+
+
+def split_by_cost(cost: Sequence[float], world: int) -> np.ndarray:
+  """Boundaries [world + 1] of contiguous chunks of ``cost`` with near-equal
+  totals (rank r takes items bounds[r]:bounds[r+1])."""
+  c = np.cumsum(np.asarray(cost, dtype=np.float64))
+  total = c[-1] if len(c) else 0.0
+  cuts = [int(np.searchsorted(c, total * r / world, side='left')) for r in range(1, world)]
+  return np.array([0] + cuts + [len(c)], dtype=np.int64)
+
+
+def sharded_sym_levels(levels_fn: Callable, lengths: Sequence[int],
+                       group: Optional['dist.ProcessGroup'] = None):
+  """Per-level values of K(X) over the upper triangle, sharded by cost.
+
+  The upper-triangle pair list is cut into contiguous chunks of equal cell
+  count (``(L_a - 1)(L_b - 1)`` per pair, so ragged batches balance), rank r
+  evaluates its chunk with ``levels_fn(pairs) -> [n_levels + 1, len(pairs)]``
+  (for a ``ksig_b200`` kernel: the level kernels of an explicit pair list),
+  and one all_gather assembles the full ``[n_levels + 1, n(n+1)/2]`` array in
+  upper-triangle order on every rank, ready for the normalisation.  Half the
+  pairs of the row-block split, and no pair twice.
+  """
+  world = dist.get_world_size(group) if dist.is_initialized() else 1
+  rank = dist.get_rank(group) if dist.is_initialized() else 0
+  n = len(lengths)
+  pairs = upper_pairs(n)
+  lx = np.maximum(np.asarray(lengths, dtype=np.float64) - 1, 1)
+  bounds = split_by_cost(lx[pairs[:, 0]] * lx[pairs[:, 1]], world)
+  mine = pairs[bounds[rank]:bounds[rank + 1]]
+  lev = torch.as_tensor(levels_fn(mine))
+  if world == 1:
+    return lev
+  counts = [int(bounds[r + 1] - bounds[r]) for r in range(world)]
+  pad = max(counts)
+  buf = lev.new_zeros((lev.shape[0], pad))
+  buf[:, :lev.shape[1]] = lev
+  parts = [torch.empty_like(buf) for _ in range(world)]
+  dist.all_gather(parts, buf, group=group)
+  return torch.cat([p[:, :c] for p, c in zip(parts, counts)], dim=1)
+
+
+def sharded_sym_gram(kernel, X, group: Optional['dist.ProcessGroup'] = None):
+  """K(X) of a ``ksig_b200`` SignatureKernel / SignaturePDEKernel with the
+  upper triangle sharded over the ranks (see :func:`sharded_sym_levels`);
+  returns the normalised ``[n, n]`` matrix on every rank."""
+  from . import _engine as E
+  from . import _lib as L
+  from .kernels import SignaturePDEKernel, _to_seqs
+  Xs, _, _ = _to_seqs(X, kernel.n_features)
+  lengths = (Xs.lengths.cpu().numpy() if Xs.lengths is not None
+             else np.full((Xs.n,), Xs.L))
+
+  def levels_fn(pairs):
+    pl = torch.as_tensor(pairs, device=Xs.data.device).contiguous()
+    kind, param = kernel._static()
+    if isinstance(kernel, SignaturePDEKernel):
+      return E.pde_values(Xs, Xs, L.PAIRS_LIST, kernel.dyadic_order, kernel.difference,
+                          kind, param, pair_list=pl)[None, :]
+    return E.sig_levels(Xs, Xs, L.PAIRS_LIST, kernel.n_levels, kernel.order,
+                        kernel.difference, kind, param, pair_list=pl)
+
+  lev = sharded_sym_levels(levels_fn, lengths, group)
+  return E.normalize_levels(lev.contiguous(), L.PAIRS_UPPER, Xs.n, Xs.n, None, None,
+                            kernel.normalize, Xs.data.dtype)

@@ -123,3 +123,59 @@ def test_sharded_gram_gradients_two_ranks_gloo():
     np.testing.assert_allclose(full, ref.detach().numpy(), rtol=1e-12)
     np.testing.assert_allclose(gx, Xt.grad.numpy(), rtol=1e-10, atol=1e-14)
     np.testing.assert_allclose(gy, Yt.grad.numpy(), rtol=1e-10, atol=1e-14)
+
+
+def test_split_by_cost_balances_and_covers():
+  from ksig_b200.distributed import split_by_cost, upper_pairs
+  p = upper_pairs(5)
+  assert p.shape == (15, 2) and (p[:, 0] <= p[:, 1]).all()
+  assert p[:5].tolist() == [[0, 0], [0, 1], [0, 2], [0, 3], [0, 4]]
+  cost = np.r_[np.ones(10), np.full(10, 9.0)]
+  b = split_by_cost(cost, 4)
+  assert b[0] == 0 and b[-1] == 20 and (np.diff(b) >= 0).all()
+  sums = [cost[b[r]:b[r + 1]].sum() for r in range(4)]
+  assert max(sums) - min(sums) <= 9.0
+
+
+def _sym_worker(rank, world, port, xs, out_q):
+  import sys
+  sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+  from oracle import ksig_oracle as O
+  from ksig_b200.distributed import sharded_sym_levels
+  os.environ['MASTER_ADDR'] = '127.0.0.1'
+  os.environ['MASTER_PORT'] = str(port)
+  dist.init_process_group('gloo', rank=rank, world_size=world)
+  try:
+    def levels_fn(pairs):
+      # One pair at a time through the oracle: [n_levels + 1, len(pairs)].
+      cols = [O.signature_kernel([xs[a]], [xs[b]], n_levels=3, return_levels=True,
+                                 param=0.7)[:, 0, 0] for a, b in pairs]
+      return torch.tensor(np.stack(cols, axis=1)) if cols else torch.zeros((4, 0), dtype=torch.float64)
+    lev = sharded_sym_levels(levels_fn, [len(x) for x in xs])
+    out_q.put((rank, lev.numpy()))
+  finally:
+    dist.destroy_process_group()
+
+
+def test_sharded_sym_levels_two_ranks_gloo():
+  """The cost-balanced upper-triangle split plus one all_gather gives every
+  rank the full per-level array in KSIG_PAIRS_UPPER order."""
+  from oracle import ksig_oracle as O
+  from ksig_b200.distributed import upper_pairs
+  rng = np.random.default_rng(2)
+  xs = [np.cumsum(rng.standard_normal((n, 2)) * 0.3, 0) for n in (4, 15, 7, 11, 3)]
+  ctx = mp.get_context('spawn')
+  q = ctx.Queue()
+  port = _free_port()
+  procs = [ctx.Process(target=_sym_worker, args=(r, 2, port, xs, q)) for r in range(2)]
+  for p in procs:
+    p.start()
+  res = [q.get(timeout=180) for _ in procs]
+  for p in procs:
+    p.join(timeout=60)
+    assert p.exitcode == 0
+  full = O.signature_kernel(xs, None, n_levels=3, return_levels=True, param=0.7)
+  pairs = upper_pairs(len(xs))
+  ref = full[:, pairs[:, 0], pairs[:, 1]]
+  for _, lev in res:
+    np.testing.assert_allclose(lev, ref, rtol=1e-12, atol=1e-14)

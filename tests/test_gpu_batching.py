@@ -157,3 +157,18 @@ def test_precompute_kernel_mat_matches_full_call(batch_size):
   np.testing.assert_allclose(got, full, rtol=1e-12, atol=1e-14)
   np.testing.assert_allclose(got2, full2, rtol=1e-12, atol=1e-14)
   np.testing.assert_allclose(got, got.T, rtol=0, atol=0)
+
+
+@pytest.mark.parametrize('pde', [False, True])
+def test_sharded_sym_gram_single_rank_equals_call(pde):
+  """The upper-triangle pair-list path (KSIG_PAIRS_LIST + normalisation of
+  the gathered triangle) reproduces K(X); with one rank it is the whole
+  triangle."""
+  import ksig_b200 as K
+  from ksig_b200.distributed import sharded_sym_gram
+  rng = np.random.default_rng(31)
+  xs = [np.cumsum(rng.standard_normal((n, 3)) * 0.3, 0) for n in (9, 30, 4, 17, 22, 2)]
+  kern = (K.SignaturePDEKernel(dyadic_order=1, static_kernel=K.RBFKernel(0.8)) if pde
+          else K.SignatureKernel(n_levels=4, order=2, static_kernel=K.RBFKernel(0.8)))
+  got = sharded_sym_gram(kern, xs).cpu().numpy()
+  np.testing.assert_allclose(got, kern(xs), rtol=1e-12, atol=1e-14)
