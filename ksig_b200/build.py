@@ -109,6 +109,8 @@ def instances():
       add(('dpb', dt, kd, c, nl, 1, 1))
     for nl, kd in itertools.product([2, 3, 4, 5, 6, 8], kds):
       add(('dpb', dt, kd, 2, nl, 2, 1))
+      if dt == 'f32' and kd in KD_FEW:
+        add(('dpb', dt, kd, 3, nl, 2, 1))  # wider order-2 strips
     for p, nls in ((3, [3, 4, 5, 6, 8]), (4, [4, 5, 6, 8])):
       for nl, kd in itertools.product(nls, KD_FEW):
         add(('dpb', dt, kd, 2, nl, p, 1))
