@@ -273,6 +273,33 @@ def run_ours(args, rank, world, dist):
       pm.append(a.elapsed_time(b))
     plain_ms = sum(pm) / len(pm)
 
+  # The adjoints on the same 512 x 512 levels: fused (skewed two-phase sweep)
+  # and plain one-pair-per-block, each on random level weights.
+  bwd_ms = plain_bwd_ms = None
+  if not args.no_plain and not args.no_bwd:
+    gl = torch.randn((N_LEVELS + 1, N_SEQ * N_SEQ), device=dev, dtype=torch.float64)
+
+    def timed_once(fn, reps):
+      out = []
+      for _ in range(reps):
+        flush.fill_(3)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        b.synchronize()
+        out.append(a.elapsed_time(b))
+      return sum(out) / len(out)
+
+    fb = lambda: E.sig_levels_bwd(Xs, Ys, Lb.PAIRS_FULL, N_LEVELS, ORDER,  # noqa: E731
+                                  Lb.STATIC_RBF, BANDWIDTH, gl, want_dparam=False)
+    fb()
+    bwd_ms = timed_once(fb, 3)
+    pb = lambda: E.sig_levels_bwd_plain(Xs, Ys, Lb.PAIRS_FULL, N_LEVELS, ORDER,  # noqa: E731
+                                        Lb.STATIC_RBF, BANDWIDTH, gl, want_dparam=False)
+    plain_bwd_ms = timed_once(pb, 1)
+
   # End to end through the public API from pinned host memory.
   Xh = torch.as_tensor(X).pin_memory()
   Yh = torch.as_tensor(Y).pin_memory()
@@ -364,8 +391,13 @@ def run_ours(args, rank, world, dist):
         'plain_fp32': None if plain_ms is None else {
             'kernel_ms': plain_ms, 'fused_kernel_ms': k_ms,
             'speedup': plain_ms / k_ms,
-            'what': 'plain FP32 one-pair-per-block kernel '
-                    '(ksig_signature_kern_plain) on the same 512x512 levels'},
+            'bwd_kernel_ms': plain_bwd_ms, 'fused_bwd_kernel_ms': bwd_ms,
+            'speedup_bwd': (plain_bwd_ms / bwd_ms) if bwd_ms else None,
+            'speedup_fwd_bwd': ((plain_ms + plain_bwd_ms) / (k_ms + bwd_ms))
+                               if bwd_ms else None,
+            'what': 'plain FP32 one-pair-per-block kernels '
+                    '(ksig_signature_kern_plain, ksig_signature_kern_plain_bwd) '
+                    'against the fused sweep and adjoint on the same 512x512 levels'},
         'fwd_bwd': None if fb_ms is None else {
             's_per_step': fb_ms * 1e-3, 'ms_per_step': fb_ms,
             'what': 'K(X, Y) forward + dL/dX backward (L = sum W*K), '
