@@ -98,6 +98,12 @@ dp_bwd_kernel(const DpBwdArgs<T> args) {
   constexpr int RV = RS / VN;
   using V = typename Vec<T>::type;
   constexpr int STRIP = 32 * C - 1;
+  // Two steps per loop trip remove the per-step register moves of the
+  // pipelined row state; only small FP32 order-1 instances take it, since
+  // on the others it raises spills (4 KD + C NL is a proxy for their
+  // register footprint).
+  constexpr int kStepUnroll =
+      (sizeof(T) == 4 && P == 1 && 4 * KD + C * NL <= 60) ? 2 : 1;
 
   extern __shared__ __align__(16) unsigned char dsm[];
   const int lane = threadIdx.x & 31;
@@ -118,6 +124,7 @@ dp_bwd_kernel(const DpBwdArgs<T> args) {
   const bool want_dpar = args.dparam != nullptr;
   const T inv2a = T(1.0 / (2.0 * alpha));
   const double xscale = rbf ? 1.0 / (args.param * args.param) : args.param;
+  const T xscale_t = T(xscale);
   double dpar_w = 0.0;
 
   for (long long tid = wg; tid < args.ntasks; tid += nw) {
@@ -198,6 +205,7 @@ dp_bwd_kernel(const DpBwdArgs<T> args) {
       const T* blin = BL + (long long)((s + 1) & 1) * rm * NX;  // written by strip s - 1
       T* blout = BL + (long long)(s & 1) * rm * NX;
       const int T1 = lx + 33;
+#pragma unroll kStepUnroll
       for (int t = 0; t < T1; ++t) {
         const int rho = t - lane;     // grid row computed this step
         const int r = rho - 2;        // cell row processed this step
@@ -361,6 +369,7 @@ dp_bwd_kernel(const DpBwdArgs<T> args) {
           recn[h] = (act0 && NH > 0) ? rec_at(s, lx + 33)[h * 32 + lane] : T(0);
       }
       const int T2 = lx + 33;
+#pragma unroll kStepUnroll
       for (int u = 0; u < T2; ++u) {
         const int rho = u - (31 - lane);
         const int g = lx - rho;                      // grid row computed; cell row processed
@@ -661,7 +670,7 @@ dp_bwd_kernel(const DpBwdArgs<T> args) {
           for (int k = 0; k < KD; ++k) {
             if (k < args.d) {
               const T v = rbf ? acc[k] - acc[KD] * (xp[k] * inv2a) : acc[k];
-              atomicAdd(dst + k, (T)(xscale * (double)v));
+              atomicAdd(dst + k, xscale_t * v);
             }
           }
         }
