@@ -99,11 +99,10 @@ dp_bwd_kernel(const DpBwdArgs<T> args) {
   using V = typename Vec<T>::type;
   constexpr int STRIP = 32 * C - 1;
   // Two steps per loop trip remove the per-step register moves of the
-  // pipelined row state; only small FP32 order-1 instances take it, since
-  // on the others it raises spills (4 KD + C NL is a proxy for their
-  // register footprint).
-  constexpr int kStepUnroll =
-      (sizeof(T) == 4 && P == 1 && 4 * KD + C * NL <= 60) ? 2 : 1;
+  // pipelined row state.  FP32 order 1 only: the order >= 2 and FP64
+  // instances hold more state per cell, and there the unrolled loop spills
+  // more and runs slower.
+  constexpr int kStepUnroll = (sizeof(T) == 4 && P == 1) ? 2 : 1;
 
   extern __shared__ __align__(16) unsigned char dsm[];
   const int lane = threadIdx.x & 31;
