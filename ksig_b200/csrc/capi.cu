@@ -293,6 +293,22 @@ int want_cols(int ly_cells, int cap, int op) {
   const int forced = env_int("KSIG_FWD_COLS", 0);
   if (forced > 0) return forced;
   static const int opts[] = {2, 4, 7, 8};
+  if (op == OP_DP_FWD) {
+    // Fewest lane-steps per row with a per-step overhead of 1.5 cells:
+    // strips * (C + 1.5), ties to the wider strip.  Fitted to B200 timings
+    // of the FP32 order-1 sweep (C = 4 beats C = 7 at 255 columns, C = 7
+    // wins at 199 and 399).
+    int best = 0;
+    long long best_cost = -1;
+    for (int c : {2, 4, 7}) {
+      if (c > cap) break;
+      const long long strip = 32 * c - 1;
+      const long long ns = ly_cells <= strip ? 1 : (ly_cells + strip - 1) / strip;
+      const long long cost = ns * (2 * c + 3);
+      if (best_cost < 0 || cost <= best_cost) { best_cost = cost; best = c; }
+    }
+    return best > 0 ? best : cap;
+  }
   for (int c : opts) {
     if (c > cap) break;
     if (32 * c - 1 >= ly_cells) return c;
