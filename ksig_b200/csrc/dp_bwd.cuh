@@ -87,9 +87,11 @@ __host__ __device__ inline size_t dp_bwd_smem_bytes(int wpb, int c, int rs, size
   return (size_t)wpb * (c + 1) * (rs * es / 16) * 32 * 16;
 }
 
-template <typename T, int KD, int C, int NL, int P, int WPB>
-__global__ void __launch_bounds__(WPB * 32)
-dp_bwd_kernel(const DpBwdArgs<T> args) {
+// Kernel body.  RBF_NOPAR: RBF static kernel and no parameter gradient,
+// known at compile time (no per-point kind tests, no distance arguments
+// kept for dparam).
+template <typename T, int KD, int C, int NL, int P, int WPB, bool RBF_NOPAR>
+__device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
   using Lay = DpLayout<NL, P>;
   constexpr int NH = Lay::NH;
   constexpr int NX = NH > 0 ? NH : 1;
@@ -119,8 +121,8 @@ dp_bwd_kernel(const DpBwdArgs<T> args) {
   T* BR = BL + 2 * rm * NX;
 
   const double alpha = 1.4426950408889634 / fmax(2.0 * args.param * args.param, 1e-12);
-  const bool rbf = args.kind == KIND_RBF;
-  const bool want_dpar = args.dparam != nullptr;
+  const bool rbf = RBF_NOPAR || args.kind == KIND_RBF;
+  const bool want_dpar = !RBF_NOPAR && args.dparam != nullptr;
   const T inv2a = T(1.0 / (2.0 * alpha));
   const double xscale = rbf ? 1.0 / (args.param * args.param) : args.param;
   const T xscale_t = T(xscale);
@@ -179,7 +181,7 @@ dp_bwd_kernel(const DpBwdArgs<T> args) {
 #pragma unroll
         for (int k = 0; k < KD; ++k) acc = fma(xv[k], yv[k], acc);
         arg[c] = acc;
-        m[c] = static_value(acc, args.kind);
+        m[c] = rbf ? kexp2(acc) : acc;
       }
     };
     auto rec_at = [&](int s, long long t) { return REC + ((long long)s * steps_max + t) * NX * 32; };
@@ -377,7 +379,7 @@ dp_bwd_kernel(const DpBwdArgs<T> args) {
         // Values lane l+1 produced one step earlier (same rows).
         const T right = shfl_down(DMlast0, 1);
         const T mr_new = shfl_down(Mprev[0], 1);
-        const T ar_new = shfl_down(argprev[0], 1);
+        const T ar_new = want_dpar ? shfl_down(argprev[0], 1) : T(0);
         T Ain[NX];
 #pragma unroll
         for (int h = 0; h < NX; ++h) Ain[h] = shfl_down(Aprev[h], 1);
@@ -696,6 +698,15 @@ dp_bwd_kernel(const DpBwdArgs<T> args) {
       atomicAdd(args.dparam, rbf ? -dpar_w / (alpha * p * p * p) : dpar_w / p);
     }
   }
+}
+
+template <typename T, int KD, int C, int NL, int P, int WPB>
+__global__ void __launch_bounds__(WPB * 32)
+dp_bwd_kernel(const DpBwdArgs<T> args) {
+  if (args.kind == KIND_RBF && args.dparam == nullptr)
+    dp_bwd_body<T, KD, C, NL, P, WPB, true>(args);
+  else
+    dp_bwd_body<T, KD, C, NL, P, WPB, false>(args);
 }
 
 }  // namespace ksig
