@@ -48,9 +48,12 @@ def instances():
   """(op, dtype, kd, c, nl, p, diff) tuples.  op: dp/pde/dpb/pdeb."""
   out = []
   add = out.append
-  # DP forward, float.
+  # DP forward, float.  No 7-column tiles above 16 coordinates: there the
+  # column points no longer fit in registers (tens of KB of spills per
+  # thread; 2.6x to 11x slower than 4 columns at L = 200 on B200).
   for nl, kd, c in itertools.product(NL_ALL, KD_ALL, [2, 4, 7]):
-    add(('dp', 'f32', kd, c, nl, 1, 1))
+    if c < 7 or kd <= 16:
+      add(('dp', 'f32', kd, c, nl, 1, 1))
   for nl, kd, c in itertools.product([2, 3, 4, 5, 6, 8], KD_ALL, [2, 4]):
     add(('dp', 'f32', kd, c, nl, 2, 1))
   for p, nls in ((3, [3, 4, 5, 6, 8]), (4, [4, 5, 6, 8])):
@@ -102,11 +105,17 @@ def instances():
     add(('dp', 'f64', kd, 2, nl, 1, 1))
     add(('dpb', 'f64', kd, 2, nl, 1, 1))
   for nl, kd, c in itertools.product([10, 12], KD_MID, [2, 4]):
-    add(('dpb', 'f32', kd, c, nl, 1, 1))
-  # DP backward (row-side gradients).
+    if c < 4 or kd <= 16:
+      add(('dpb', 'f32', kd, c, nl, 1, 1))
+  # DP backward (row-side gradients).  The adjoint holds more per-column
+  # state than the forward: 7-column tiles only up to 12 coordinates and
+  # 4-column tiles up to 16 (beyond that they spill heavily; measured on
+  # B200, d = 16: 4 columns 1.1-1.6x faster than 7; d = 32: 2 columns 1.7x
+  # faster than 4 and 13x faster than 7).
   for dt, cs, kds in (('f32', [2, 4, 7], KD_MID), ('f64', [2], KD_FEW)):
     for nl, kd, c in itertools.product(NL_ALL, kds, cs):
-      add(('dpb', dt, kd, c, nl, 1, 1))
+      if c == 2 or (c == 4 and kd <= 16) or (c == 7 and kd <= 12):
+        add(('dpb', dt, kd, c, nl, 1, 1))
     for nl, kd in itertools.product([2, 3, 4, 5, 6, 8], kds):
       add(('dpb', dt, kd, 2, nl, 2, 1))
       if dt == 'f32' and kd in KD_FEW:

@@ -48,6 +48,45 @@ template <> struct Vec<double> { using type = double2; static constexpr int N = 
 __device__ __forceinline__ float kexp2(float a) { return exp2f(a); }
 __device__ __forceinline__ double kexp2(double a) { return exp2(a); }
 
+// Fused-Gram argument of two packed rows, x[KD] + y[KD] + sum_{k<KD} x[k] y[k]
+// (the packed format: norms at index KD, zero padding after it).  PAIR (FP32,
+// KD >= 5) uses paired FP32 instructions (FFMA2: two fused multiply-adds per
+// issue, each rounded like fmaf) over coordinate pairs (2j, 2j+1), summed in
+// two interleaved chains that meet at the end.  It saves issue slots but
+// can raise register use, so the kernels enable it per instantiation where
+// their occupancy stays the same.
+template <int KD, bool PAIR, typename XA, typename YA>
+__device__ __forceinline__ float packed_arg(const XA& x, const YA& y, float) {
+  if constexpr (PAIR && KD >= 5) {
+    float2 s;
+    if constexpr (KD % 2 == 1) {
+      s = make_float2(x[KD] + y[KD], x[KD - 1] * y[KD - 1]);
+#pragma unroll
+      for (int j = 0; j < KD / 2; ++j)
+        s = __ffma2_rn(make_float2(x[2 * j], x[2 * j + 1]), make_float2(y[2 * j], y[2 * j + 1]), s);
+      return s.x + s.y;
+    } else {
+      s = __fmul2_rn(make_float2(x[0], x[1]), make_float2(y[0], y[1]));
+#pragma unroll
+      for (int j = 1; j < KD / 2; ++j)
+        s = __ffma2_rn(make_float2(x[2 * j], x[2 * j + 1]), make_float2(y[2 * j], y[2 * j + 1]), s);
+      return s.x + (s.y + (x[KD] + y[KD]));
+    }
+  } else {
+    float acc = x[KD] + y[KD];
+#pragma unroll
+    for (int k = 0; k < KD; ++k) acc = fmaf(x[k], y[k], acc);
+    return acc;
+  }
+}
+template <int KD, bool PAIR, typename XA, typename YA>
+__device__ __forceinline__ double packed_arg(const XA& x, const YA& y, double) {
+  double acc = x[KD] + y[KD];
+#pragma unroll
+  for (int k = 0; k < KD; ++k) acc = fma(x[k], y[k], acc);
+  return acc;
+}
+
 // Static kernel value from the fused dot-product argument (RBF, linear).
 template <typename T>
 __device__ __forceinline__ T static_value(T arg, int kind) {

@@ -105,6 +105,8 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
   // instances hold more state per cell, and there the unrolled loop spills
   // more and runs slower.
   constexpr int kStepUnroll = (sizeof(T) == 4 && P == 1) ? 2 : 1;
+  // Paired FP32 Gram arguments (packed_arg) where they keep the occupancy.
+  constexpr bool kPairArg = sizeof(T) == 4 && KD <= 16 && (C >= 7 || P >= 2);
 
   extern __shared__ __align__(16) unsigned char dsm[];
   const int lane = threadIdx.x & 31;
@@ -177,9 +179,7 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
       for (int c = 0; c < C; ++c) {
         T yv[RS];
         y_col(c, yv);
-        T acc = xv[KD] + yv[KD];
-#pragma unroll
-        for (int k = 0; k < KD; ++k) acc = fma(xv[k], yv[k], acc);
+        const T acc = packed_arg<KD, kPairArg>(xv, yv, T(0));
         arg[c] = acc;
         m[c] = rbf ? kexp2(acc) : acc;
       }

@@ -159,9 +159,7 @@ pde_bwd_kernel(const PdeBwdArgs<T> args) {
       for (int v = 0; v < RS / VN; ++v) reinterpret_cast<V*>(xv)[v] = __ldg(p + v);
 #pragma unroll
       for (int c = 0; c <= C; ++c) {
-        T acc = xv[KD] + yv[c][KD];
-#pragma unroll
-        for (int k = 0; k < KD; ++k) acc = fma(xv[k], yv[c][k], acc);
+        const T acc = packed_arg<KD, false>(xv, yv[c], T(0));
         arg[c] = acc;
         m[c] = static_value(acc, args.kind);
       }

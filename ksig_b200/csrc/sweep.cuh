@@ -80,6 +80,7 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
   constexpr int VN = Vec<T>::N;
   using V = typename Vec<T>::type;
   constexpr int STRIP = DIFF ? 32 * C - 1 : 32 * C;
+  constexpr bool kPairArg = Policy::kPairArg && KD <= 16;
 
   const int lane = threadIdx.x & 31;
   const long long wg = (long long)blockIdx.x * WPB + (threadIdx.x >> 5);
@@ -168,9 +169,7 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
   auto gram = [&](bool RBF, const T (&xv)[RS], T (&m)[C]) {
 #pragma unroll
     for (int c = 0; c < C; ++c) {
-      T acc = xv[KD] + yv[c][KD];
-#pragma unroll
-      for (int k = 0; k < KD; ++k) acc = fma(xv[k], yv[c][k], acc);
+      const T acc = packed_arg<KD, kPairArg>(xv, yv[c], T(0));
       m[c] = RBF ? kexp2(acc) : acc;
     }
   };
@@ -197,9 +196,7 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
         }
         m[c] = static_value_other(acc, args.kind, args.sp);
       } else {
-        T acc = xv[KD] + yv[c][KD];
-#pragma unroll
-        for (int k = 0; k < KD; ++k) acc = fma(xv[k], yv[c][k], acc);
+        const T acc = packed_arg<KD, kPairArg>(xv, yv[c], T(0));
         m[c] = static_value(acc, args.kind);
       }
     }
@@ -490,6 +487,9 @@ struct DpPolicy {
   // Two-step unrolling of the steady loop only while the register state is
   // small enough not to spill.
   static constexpr bool kUnroll2 = P == 1 && (NX + 3) * C <= 40 && sizeof(T) == 4;
+  // Paired FP32 Gram arguments (packed_arg): the wide strips of the deeper
+  // truncations, where the register count and occupancy stay the same.
+  static constexpr bool kPairArg = sizeof(T) == 4 && C >= 7 && NL >= 5;
   T X[NX];                    // horizontal running sums (outgoing)
   T Ccol[NX][C];              // column running sums
   T Clast[C];                 // column sums of the last level's totals
@@ -680,6 +680,7 @@ template <typename T, int C, int F, bool DIFF>
 struct PdePolicy {
   static constexpr int NX = 2 * F;
   static constexpr bool kUnroll2 = C * F <= 16 && sizeof(T) == 4;
+  static constexpr bool kPairArg = false;
   static constexpr int STRIP = DIFF ? 32 * C - 1 : 32 * C;
   T X[NX];
   T Kr[C * F];
@@ -809,6 +810,7 @@ template <typename T, int C>
 struct GaPolicy {
   static constexpr int NX = 1;
   static constexpr bool kUnroll2 = false;
+  static constexpr bool kPairArg = false;
   static constexpr int STRIP = 32 * C;
   T X[NX];
   T Kr[C];       // logK of the row above, the lane's columns
