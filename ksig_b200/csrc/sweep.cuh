@@ -488,8 +488,9 @@ struct DpPolicy {
   // small enough not to spill.
   static constexpr bool kUnroll2 = P == 1 && (NX + 3) * C <= 40 && sizeof(T) == 4;
   // Paired FP32 Gram arguments (packed_arg): the wide strips of the deeper
-  // truncations, where the register count and occupancy stay the same.
-  static constexpr bool kPairArg = sizeof(T) == 4 && C >= 7 && NL >= 5;
+  // truncations and the 4-column higher-order tiles, where the register
+  // count and occupancy stay the same.
+  static constexpr bool kPairArg = sizeof(T) == 4 && NL >= 5 && (C >= 7 || (P >= 2 && C >= 4));
   T X[NX];                    // horizontal running sums (outgoing)
   T Ccol[NX][C];              // column running sums
   T Clast[C];                 // column sums of the last level's totals
