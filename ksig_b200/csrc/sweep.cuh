@@ -594,8 +594,40 @@ struct DpPolicy {
     T H[NX];
 #pragma unroll
     for (int h = 0; h < NX; ++h) H[h] = Xin[h];
+    int c0 = 0;
+    if constexpr (kPairArg && P == 1 && NL >= 2) {
+      // Cells c and c+1 update different column sums, so once both cells'
+      // horizontal prefixes are known their column-sum updates run as paired
+      // FP32 instructions (same roundings as the scalar code below).
 #pragma unroll
-    for (int c = 0; c < C; ++c) {
+      for (int c = 0; c + 1 < C; c += 2) {
+        T h0[NX], h1[NX];
+#pragma unroll
+        for (int k = 2; k <= NL; ++k) {
+          h0[k - 2] = H[k - 2];
+          H[k - 2] += Ccol[k - 2][c];
+          h1[k - 2] = H[k - 2];
+          H[k - 2] += Ccol[k - 2][c + 1];
+        }
+        const float2 zz = make_float2(Z[c], Z[c + 1]);
+        float2 r = __fadd2_rn(make_float2(Ccol[0][c], Ccol[0][c + 1]), zz);
+        Ccol[0][c] = r.x;
+        Ccol[0][c + 1] = r.y;
+#pragma unroll
+        for (int k = 2; k < NL; ++k) {
+          r = __ffma2_rn(zz, make_float2(h0[k - 2], h1[k - 2]),
+                         make_float2(Ccol[k - 1][c], Ccol[k - 1][c + 1]));
+          Ccol[k - 1][c] = r.x;
+          Ccol[k - 1][c + 1] = r.y;
+        }
+        r = __ffma2_rn(zz, make_float2(h0[NL - 2], h1[NL - 2]), make_float2(Clast[c], Clast[c + 1]));
+        Clast[c] = r.x;
+        Clast[c + 1] = r.y;
+      }
+      c0 = C & ~1;
+    }
+#pragma unroll
+    for (int c = c0; c < C; ++c) {
       const T z = Z[c];
       T Hold[NX];
 #pragma unroll
