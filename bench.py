@@ -28,6 +28,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -108,7 +109,9 @@ class ClockSampler:
 
   def start(self):
     try:
-      out_dir = os.path.join(ROOT, 'gpurun_out')
+      # Raw samples go to KSIG_CLOCKS_DIR (default: the system temp dir);
+      # the JSON line carries their summary.
+      out_dir = os.environ.get('KSIG_CLOCKS_DIR') or tempfile.gettempdir()
       os.makedirs(out_dir, exist_ok=True)
       self.path = os.path.join(out_dir, f'clocks_gpu{self.idx}.csv')
       self.f = open(self.path, 'w')

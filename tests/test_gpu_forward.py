@@ -3,7 +3,7 @@
 Tolerances (relative, per result): FP64 inputs run FP64 kernels and must
 match the reference goldens to 1e-9; FP32 inputs must match the FP64 oracle
 on the same (FP32-rounded) inputs to 1e-5 for the DP kernel and 1e-4 for the
-PDE kernel, the bars the north-star sets for the mixed-precision path.
+PDE kernel, the bars set for the mixed-precision path.
 """
 import numpy as np
 import pytest

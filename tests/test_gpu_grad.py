@@ -1,7 +1,7 @@
 """Gradients of the CUDA adjoint against autograd through the FP64 torch
 oracle (itself pinned to central finite differences in
 tests/test_oracle_grad.py).  Tolerance: 1e-4 relative for FP32 inputs (the
-north-star bar for gradients), 1e-8 for FP64 inputs."""
+required bar for gradients), 1e-8 for FP64 inputs."""
 import numpy as np
 import pytest
 import torch
