@@ -358,3 +358,22 @@ def test_deep_truncation_levels(n_levels):
                  O.signature_kernel(X.astype(np.float32).astype(np.float64),
                                     Y.astype(np.float32).astype(np.float64),
                                     n_levels=n_levels, normalize=True, param=0.7)) < DP_TOL
+
+
+@pytest.mark.parametrize('d', [5, 7, 10, 11, 15])
+@pytest.mark.parametrize('order', [1, 2])
+def test_paired_gram_widths_fp32(d, order):
+  """FP32 instances whose Gram runs as paired FFMA2 over coordinate pairs
+  (7-column order-1 and 4-column order-2 tiles with n_levels >= 5): odd and
+  even padded widths (6, 8, 10, 12, 16)."""
+  import ksig_b200 as K
+  rng = np.random.default_rng(700 + d + 10 * order)
+  X = _walks(rng, 3, 200, d, time=False)
+  Y = _walks(rng, 2, 190, d, time=False)
+  bw = float(np.sqrt(d))
+  k = K.SignatureKernel(n_levels=5, order=order, normalize=True,
+                        static_kernel=K.RBFKernel(bw))
+  X32, Y32 = X.astype(np.float32), Y.astype(np.float32)
+  ref = O.signature_kernel(X32.astype(np.float64), Y32.astype(np.float64),
+                           n_levels=5, order=order, param=bw)
+  assert _relerr(k(X32, Y32), ref) < DP_TOL
