@@ -279,6 +279,44 @@ int ksig_signature_kern_bwd(const void* X, const int32_t* lenX, int nX,
                             double* dparam, void* workspace,
                             size_t workspace_bytes, void* stream);
 
+/*
+ * Split gradient pass (no reference counterpart: the reference has no
+ * gradients).  The same result as ksig_signature_kern (levels) followed by
+ * ksig_signature_kern_bwd (dX, dparam), in two calls that share one
+ * workspace: ksig_signature_kern_rec_fwd writes the level kernels
+ * ([n_levels + 1, P] float64, level 0 = 1) and keeps, per pair, the records
+ * the adjoint needs; ksig_signature_kern_rec_bwd then runs only the adjoint
+ * pass.  An autograd forward pays for the records once instead of
+ * recomputing the forward recursion in the backward.  The workspace
+ * (ksig_signature_kern_rec_workspace bytes: the adjoint's own plus the
+ * records, about (L + 33) * n_levels * 128 B per pair in FP32) must stay
+ * untouched between the two calls, which take the same arguments.  Order 1
+ * (after clamping), n_levels >= 2, difference 1, KSIG_PAIRS_FULL or
+ * KSIG_PAIRS_LIST only; ksig_signature_kern_rec_workspace returns 0
+ * otherwise.
+ */
+size_t ksig_signature_kern_rec_workspace(int nX, int LX, int nY, int LY,
+                                         int d, int dtype, int n_levels,
+                                         int order, int difference,
+                                         int pairs_mode, int n_list);
+int ksig_signature_kern_rec_fwd(const void* X, const int32_t* lenX, int nX,
+                                int LX, const void* Y, const int32_t* lenY,
+                                int nY, int LY, int d, int dtype,
+                                int static_kind, double static_param,
+                                int n_levels, int order, int difference,
+                                int pairs_mode, const int32_t* pair_list,
+                                int n_list, double* levels, void* workspace,
+                                size_t workspace_bytes, void* stream);
+int ksig_signature_kern_rec_bwd(const void* X, const int32_t* lenX, int nX,
+                                int LX, const void* Y, const int32_t* lenY,
+                                int nY, int LY, int d, int dtype,
+                                int static_kind, double static_param,
+                                int n_levels, int order, int difference,
+                                int pairs_mode, const int32_t* pair_list,
+                                int n_list, const double* grad_levels,
+                                void* dX, double* dparam, void* workspace,
+                                size_t workspace_bytes, void* stream);
+
 /* Workspace (bytes) required by ksig_signature_kern_pde_bwd. */
 size_t ksig_signature_kern_pde_bwd_workspace(int nX, int LX, int nY, int LY,
                                              int d, int dtype,

@@ -56,13 +56,24 @@ class SigKernelFn(torch.autograd.Function):
                              spec['normalize'], out_dtype)
       dx = dy = None
     else:
-      lev = lev_fn(Xs, Ys, L.PAIRS_FULL)
+      # Split gradient pass: the forward keeps the adjoint's records, the
+      # backward replays them (see SignatureKernel._split_pass).
+      rec = None
+      split = spec.get('rec_fn')
+      if split is not None and (Xt is not None or pt is not None):
+        rec = split[0](Xs, Ys)
+      if rec is not None:
+        lev, ctx.rec_ws = rec
+      else:
+        lev = lev_fn(Xs, Ys, L.PAIRS_FULL)
       dx = dy = None
       if spec['normalize']:
         dx = lev_fn(Xs, None, L.PAIRS_DIAG)
         dy = lev_fn(Ys, None, L.PAIRS_DIAG)
       K = E.normalize_levels(lev, L.PAIRS_FULL, Xs.n, Ys.n, dx, dy,
                              spec['normalize'], out_dtype)
+    if not hasattr(ctx, 'rec_ws'):
+      ctx.rec_ws = None
     ctx.spec = spec
     ctx.sym = sym
     ctx.saved = (lev, dx, dy)
@@ -114,7 +125,11 @@ class SigKernelFn(torch.autograd.Function):
           dpar_total += 0.5 * dp
     else:
       if want_x or want_p:
-        dXd, dp = bwd(Xs, Ys, L.PAIRS_FULL, gK.reshape(n_lev, -1), want_p)
+        if ctx.rec_ws is not None:
+          dXd, dp = spec['rec_fn'][1](Xs, Ys, gK.reshape(n_lev, -1), want_p,
+                                      ctx.rec_ws)
+        else:
+          dXd, dp = bwd(Xs, Ys, L.PAIRS_FULL, gK.reshape(n_lev, -1), want_p)
         dX = dXd
         if dp is not None:
           dpar_total += dp
@@ -134,6 +149,7 @@ class SigKernelFn(torch.autograd.Function):
             dY = dYd2 if dY is None else dY + dYd2
           if dp is not None:
             dpar_total += 0.5 * dp
+    ctx.rec_ws = None  # the records are used once
     gx = gy = None
     if want_x and dX is not None and ctx.x_meta is not None:
       shape, dtype, device = ctx.x_meta

@@ -5,6 +5,7 @@ arithmetic step runs in ``libksig_b200.so``.
 """
 
 import ctypes
+import os
 
 import numpy as np
 import torch
@@ -183,6 +184,64 @@ def sig_levels_bwd(X, Y, mode, n_levels, order, kind, param, grad_levels,
       _ptr(Yv.lengths), Yv.n, Yv.L, X.d, dt, kind, float(param), n_levels,
       order, 1, mode, _ptr(pair_list), n_list, _ptr(gl), _ptr(dX),
       _ptr(dpar), _ptr(ws), ws_bytes, _stream())
+  L.check(rc)
+  _fold_status(ws)
+  return dX, dpar
+
+
+def rec_budget_bytes(device):
+  """Memory the split gradient pass may keep for its records:
+  ``KSIG_REC_MB`` (default 65536), at most half of the free device memory."""
+  cap = int(os.environ.get('KSIG_REC_MB', '65536')) << 20
+  free, _ = torch.cuda.mem_get_info(device)
+  return min(cap, free // 2)
+
+
+def sig_levels_rec(X, Y, n_levels, order, kind, param, pair_list=None):
+  """Forward of the split gradient pass (order 1): per-level kernels
+  ``[n_levels+1, P]`` (float64) and the workspace holding the records of
+  :func:`sig_levels_bwd_rec`, or None when the pass does not apply or its
+  records exceed :func:`rec_budget_bytes`."""
+  lib = L.lib()
+  dt = _dtype_code(X.data)
+  mode = L.PAIRS_FULL if pair_list is None else L.PAIRS_LIST
+  n_list = 0 if pair_list is None else pair_list.shape[0]
+  ws_bytes = lib.ksig_signature_kern_rec_workspace(
+      X.n, X.L, Y.n, Y.L, X.d, dt, n_levels, order, 1, mode, n_list)
+  if ws_bytes == 0 or ws_bytes > rec_budget_bytes(X.data.device):
+    return None
+  P = num_pairs(mode, X.n, Y.n, n_list)
+  out = torch.empty((n_levels + 1, max(P, 0)), dtype=torch.float64,
+                    device=X.data.device)
+  ws = _workspace(ws_bytes, X.data.device)
+  rc = lib.ksig_signature_kern_rec_fwd(
+      _ptr(X.data), _ptr(X.lengths), X.n, X.L, _ptr(Y.data), _ptr(Y.lengths),
+      Y.n, Y.L, X.d, dt, kind, float(param), n_levels, order, 1, mode,
+      _ptr(pair_list), n_list, _ptr(out), _ptr(ws), ws_bytes, _stream())
+  L.check(rc)
+  _fold_status(ws)
+  return out, ws
+
+
+def sig_levels_bwd_rec(X, Y, n_levels, order, kind, param, grad_levels, ws,
+                       dX=None, want_dparam=True, pair_list=None):
+  """Adjoint pass of the split gradient pass: the records left in ``ws`` by
+  :func:`sig_levels_rec` (same arguments) replace the forward recursion.
+  Returns ``(dX, dparam)`` like :func:`sig_levels_bwd`."""
+  lib = L.lib()
+  dt = _dtype_code(X.data)
+  mode = L.PAIRS_FULL if pair_list is None else L.PAIRS_LIST
+  n_list = 0 if pair_list is None else pair_list.shape[0]
+  if dX is None:
+    dX = torch.zeros_like(X.data)
+  dpar = torch.zeros((1,), dtype=torch.float64, device=X.data.device) \
+      if want_dparam else None
+  gl = grad_levels.to(torch.float64).contiguous()
+  rc = lib.ksig_signature_kern_rec_bwd(
+      _ptr(X.data), _ptr(X.lengths), X.n, X.L, _ptr(Y.data), _ptr(Y.lengths),
+      Y.n, Y.L, X.d, dt, kind, float(param), n_levels, order, 1, mode,
+      _ptr(pair_list), n_list, _ptr(gl), _ptr(dX), _ptr(dpar), _ptr(ws),
+      ws.numel(), _stream())
   L.check(rc)
   _fold_status(ws)
   return dX, dpar

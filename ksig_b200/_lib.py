@@ -60,6 +60,13 @@ _SIGNATURES = {
     'ksig_signature_kern_bwd': (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _I, _I,
                                      _I, _D, _I, _I, _I, _I, _P, _I, _P, _P,
                                      _P, _P, _SZ, _P]),
+    'ksig_signature_kern_rec_workspace': (_SZ, [_I] * 11),
+    'ksig_signature_kern_rec_fwd': (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _I,
+                                         _I, _I, _D, _I, _I, _I, _I, _P, _I,
+                                         _P, _P, _SZ, _P]),
+    'ksig_signature_kern_rec_bwd': (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _I,
+                                         _I, _I, _D, _I, _I, _I, _I, _P, _I,
+                                         _P, _P, _P, _P, _SZ, _P]),
     'ksig_signature_kern_pde_bwd_workspace': (_SZ, [_I] * 10),
     'ksig_signature_kern_pde_bwd': (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _I,
                                          _I, _I, _D, _I, _I, _I, _P, _I, _P,

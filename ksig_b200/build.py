@@ -129,6 +129,10 @@ def instances():
     for p, nls in ((3, [3, 4, 5, 6, 8]), (4, [4, 5, 6, 8])):
       for nl, kd in itertools.product(nls, KD_FEW):
         add(('dpb', dt, kd, 2, nl, p, 1))
+  # Forward pass of the split gradient pass: one per order-1 adjoint tile
+  # with at least two levels (same tile, same records).
+  out += [('dpr',) + inst[1:] for inst in out
+          if inst[0] == 'dpb' and inst[5] == 1 and inst[4] >= 2]
   return out
 
 
@@ -139,6 +143,7 @@ OPS = {
     'pdex': ('OP_PDE_FWD_EXT', 'pde_fwd_kernel<{T}, {kd}, {c}, {p}, {diff}, {wpb}, true>'),
     'ga': ('OP_GA_FWD', 'ga_fwd_kernel<{T}, {kd}, {c}, {wpb}>'),
     'dpb': ('OP_DP_BWD', 'dp_bwd_kernel<{T}, {kd}, {c}, {nl}, {p}, {wpb}>'),
+    'dpr': ('OP_DP_REC_FWD', 'dp_rec_fwd_kernel<{T}, {kd}, {c}, {nl}, {p}, {wpb}>'),
     'pdeb': ('OP_PDE_BWD', 'pde_bwd_kernel<{T}, {kd}, {c}, {p}, {wpb}>'),
 }
 

@@ -483,6 +483,7 @@ struct BwdPlan {
   size_t dyn_smem;
   long long scratch_per_warp;
   size_t off_scratch, total;
+  long long rec_per_pair;  // split pass: record elements kept per pair
 };
 
 int plan_bwd(int nX, int LX, int nY, int LY, int d, int dtype, int n_levels, int order,
@@ -534,6 +535,10 @@ int plan_bwd(int nX, int LX, int nY, int LY, int d, int dtype, int n_levels, int
   long long warps = (long long)sms * occ * k->wpb;
   if (warps > bp.f.ntasks) warps = bp.f.ntasks > 0 ? bp.f.ntasks : 1;
   bp.scratch_per_warp = dp_bwd_scratch_elems(bp.ns_max, bp.rows_max, bp.nx, bp.c);
+  // Records + final column sums of one pair (the REC and CS regions of the
+  // per-warp scratch), padded to 16 bytes.
+  bp.rec_per_pair = ((long long)bp.ns_max * (bp.rows_max + 33) * bp.nx * 32 +
+                     (long long)bp.ns_max * bp.nx * bp.c * 32 + 3) / 4 * 4;
   // The per-step records grow with the strip count and the row count; keep
   // the whole scratch within a bounded budget by running fewer warps.
   const long long budget = (long long)env_int("KSIG_DP_BWD_SCRATCH_MB", 32768) << 20;
@@ -546,11 +551,19 @@ int plan_bwd(int nX, int LX, int nY, int LY, int d, int dtype, int n_levels, int
   return KSIG_OK;
 }
 
+// The split forward pass compiled for the same tile as the plan's adjoint.
+const KernelEntry* rec_fwd_entry(const BwdPlan& bp) {
+  const KernelEntry* e = find_kernel(OP_DP_REC_FWD, bp.f.f64, bp.k->kd, bp.c, bp.k->nl, 1, 1);
+  if (!e || e->kd != bp.k->kd || e->c != bp.c || e->nl != bp.k->nl) return nullptr;
+  return e;
+}
+
 template <typename T>
 int run_bwd(const BwdPlan& bp, const void* X, const int32_t* lenX, int nX, int LX,
             const void* Y, const int32_t* lenY, int nY, int LY, int d, int src_f64, int kind,
             double param, int mode, const int32_t* list, const double* glev, int nl_out,
-            void* dX, double* dparam, char* ws, cudaStream_t st) {
+            void* dX, double* dparam, char* ws, cudaStream_t st, int phases = 3,
+            double* lev = nullptr) {
   const FwdPlan& pl = bp.f;
   int* status = reinterpret_cast<int*>(ws + pl.off_status);
   T* xr = reinterpret_cast<T*>(ws + pl.off_xr);
@@ -590,8 +603,22 @@ int run_bwd(const BwdPlan& bp, const void* X, const int32_t* lenX, int nX, int L
   a.ns_max = bp.ns_max;
   a.rows_max = bp.rows_max;
   a.status = status;
+  a.phases = phases;
+  if (phases != 3) {  // split pass: records per pair, after the plan's regions
+    a.rec = reinterpret_cast<T*>(ws + bp.total);
+    a.rec_per_pair = bp.rec_per_pair;
+  }
+  a.lev = lev;
+  const void* func = bp.k->func;
+  if (phases == 1) {
+    const KernelEntry* e = rec_fwd_entry(bp);
+    if (!e) return fail(KSIG_ERR_UNSUPPORTED, "no compiled split forward pass for this tile");
+    cudaError_t ce = ensure_smem_attr(e->func, bp.dyn_smem);
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaFuncSetAttribute(split forward pass)");
+    func = e->func;
+  }
   void* kargs[] = {&a};
-  KSIG_CUDA(launch_main(bp.k->func, dim3(bp.grid), dim3(bp.k->wpb * 32), kargs, bp.dyn_smem, st));
+  KSIG_CUDA(launch_main(func, dim3(bp.grid), dim3(bp.k->wpb * 32), kargs, bp.dyn_smem, st));
   return KSIG_OK;
 }
 
@@ -1253,6 +1280,95 @@ int ksig_signature_kern_bwd(const void* X, const int32_t* lenX, int nX, int LX, 
   return run_bwd<float>(bp, X, lenX, nX, LX, Y, lenY, nY, LY, d, 0, static_kind, static_param,
                         pairs_mode, pair_list, grad_levels, n_levels, dX, dparam,
                         static_cast<char*>(workspace), st);
+}
+
+// Split gradient pass (order 1): the forward pass of the adjoint kernel
+// with its per-pair records kept in the workspace, then the adjoint pass
+// replaying them.  One plan serves both calls.
+static int rec_plan(int nX, int LX, int nY, int LY, int d, int dtype, int n_levels, int order,
+                    int difference, int pairs_mode, int n_list, BwdPlan& bp, size_t& total) {
+  if (pairs_mode != KSIG_PAIRS_FULL && pairs_mode != KSIG_PAIRS_LIST)
+    return fail(KSIG_ERR_UNSUPPORTED, "the split gradient pass takes full or listed pairs");
+  int rc = plan_bwd(nX, LX, nY, LY, d, dtype, n_levels, order, difference, pairs_mode, n_list, bp);
+  if (rc) return rc;
+  if (bp.f.p != 1 || n_levels < 2)
+    return fail(KSIG_ERR_UNSUPPORTED, "the split gradient pass needs order 1 and n_levels >= 2");
+  if (!rec_fwd_entry(bp))
+    return fail(KSIG_ERR_UNSUPPORTED, "no compiled split forward pass for this tile");
+  const size_t es = bp.f.f64 ? 8 : 4;
+  total = align_up(bp.total + (size_t)bp.f.ntasks * (size_t)bp.rec_per_pair * es);
+  return KSIG_OK;
+}
+
+size_t ksig_signature_kern_rec_workspace(int nX, int LX, int nY, int LY, int d, int dtype,
+                                         int n_levels, int order, int difference,
+                                         int pairs_mode, int n_list) {
+  BwdPlan bp;
+  size_t total = 0;
+  if (rec_plan(nX, LX, nY, LY, d, dtype, n_levels, order, difference, pairs_mode, n_list, bp,
+               total))
+    return 0;
+  return total;
+}
+
+int ksig_signature_kern_rec_fwd(const void* X, const int32_t* lenX, int nX, int LX,
+                                const void* Y, const int32_t* lenY, int nY, int LY, int d,
+                                int dtype, int static_kind, double static_param, int n_levels,
+                                int order, int difference, int pairs_mode,
+                                const int32_t* pair_list, int n_list, double* levels,
+                                void* workspace, size_t workspace_bytes, void* stream) {
+  int rc = check_common(X, Y, pairs_mode, pair_list, n_list, static_kind, static_param);
+  if (rc) return rc;
+  if (!levels) return fail(KSIG_ERR_INVALID, "levels is NULL");
+  BwdPlan bp;
+  size_t total = 0;
+  rc = rec_plan(nX, LX, nY, LY, d, dtype, n_levels, order, difference, pairs_mode, n_list, bp,
+                total);
+  if (rc) return rc;
+  if (!workspace || workspace_bytes < total)
+    return fail(KSIG_ERR_WORKSPACE, "workspace of %zu bytes is smaller than the %zu required",
+                workspace_bytes, total);
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  KSIG_CUDA(cudaMemsetAsync(workspace, 0, 16, st));
+  KSIG_CUDA(cudaMemsetAsync(levels, 0, sizeof(double) * (size_t)(n_levels + 1) * bp.f.ntasks, st));
+  if (bp.f.ntasks == 0) return KSIG_OK;
+  char* ws = static_cast<char*>(workspace);
+  if (dtype == KSIG_DTYPE_F64)
+    return run_bwd<double>(bp, X, lenX, nX, LX, Y, lenY, nY, LY, d, 1, static_kind, static_param,
+                           pairs_mode, pair_list, nullptr, n_levels, nullptr, nullptr, ws, st, 1,
+                           levels);
+  return run_bwd<float>(bp, X, lenX, nX, LX, Y, lenY, nY, LY, d, 0, static_kind, static_param,
+                        pairs_mode, pair_list, nullptr, n_levels, nullptr, nullptr, ws, st, 1,
+                        levels);
+}
+
+int ksig_signature_kern_rec_bwd(const void* X, const int32_t* lenX, int nX, int LX,
+                                const void* Y, const int32_t* lenY, int nY, int LY, int d,
+                                int dtype, int static_kind, double static_param, int n_levels,
+                                int order, int difference, int pairs_mode,
+                                const int32_t* pair_list, int n_list, const double* grad_levels,
+                                void* dX, double* dparam, void* workspace,
+                                size_t workspace_bytes, void* stream) {
+  int rc = check_common(X, Y, pairs_mode, pair_list, n_list, static_kind, static_param);
+  if (rc) return rc;
+  if (!grad_levels || !dX) return fail(KSIG_ERR_INVALID, "grad_levels / dX is NULL");
+  BwdPlan bp;
+  size_t total = 0;
+  rc = rec_plan(nX, LX, nY, LY, d, dtype, n_levels, order, difference, pairs_mode, n_list, bp,
+                total);
+  if (rc) return rc;
+  if (!workspace || workspace_bytes < total)
+    return fail(KSIG_ERR_WORKSPACE, "workspace of %zu bytes is smaller than the %zu required",
+                workspace_bytes, total);
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  KSIG_CUDA(cudaMemsetAsync(workspace, 0, 16, st));
+  if (bp.f.ntasks == 0) return KSIG_OK;
+  char* ws = static_cast<char*>(workspace);
+  if (dtype == KSIG_DTYPE_F64)
+    return run_bwd<double>(bp, X, lenX, nX, LX, Y, lenY, nY, LY, d, 1, static_kind, static_param,
+                           pairs_mode, pair_list, grad_levels, n_levels, dX, dparam, ws, st, 2);
+  return run_bwd<float>(bp, X, lenX, nX, LX, Y, lenY, nY, LY, d, 0, static_kind, static_param,
+                        pairs_mode, pair_list, grad_levels, n_levels, dX, dparam, ws, st, 2);
 }
 
 size_t ksig_signature_kern_pde_bwd_workspace(int nX, int LX, int nY, int LY, int d, int dtype,

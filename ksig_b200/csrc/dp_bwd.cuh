@@ -67,6 +67,15 @@ struct DpBwdArgs {
   long long scratch_per_warp;
   int ns_max, rows_max;
   int* status;
+  // Split gradient pass (order 1): phases 1 = forward pass only, writing the
+  // level totals to `lev` ([nl_out + 1, ntasks]); 2 = adjoint pass only,
+  // replaying the records a phase-1 launch left in `rec`; 0 or 3 = both in
+  // one launch.  `rec`: records per pair (rec_per_pair elements each) instead
+  // of per warp.
+  int phases;
+  T* rec;
+  long long rec_per_pair;
+  double* lev;
 };
 
 // Scratch elements per warp:
@@ -90,7 +99,7 @@ __host__ __device__ inline size_t dp_bwd_smem_bytes(int wpb, int c, int rs, size
 // Kernel body.  RBF_NOPAR: RBF static kernel and no parameter gradient,
 // known at compile time (no per-point kind tests, no distance arguments
 // kept for dparam).
-template <typename T, int KD, int C, int NL, int P, int WPB, bool RBF_NOPAR>
+template <typename T, int KD, int C, int NL, int P, int WPB, bool RBF_NOPAR, bool FWD_ONLY>
 __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
   using Lay = DpLayout<NL, P>;
   constexpr int NH = Lay::NH;
@@ -117,10 +126,11 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
   T* scr = args.scratch + wg * args.scratch_per_warp;
   const long long steps_max = (long long)args.rows_max + 33;
   const long long rm = args.rows_max;
-  T* REC = scr;
-  T* CS = REC + (long long)args.ns_max * steps_max * NX * 32;
-  T* BL = CS + (long long)args.ns_max * NX * C * 32;
+  const long long cs_off = (long long)args.ns_max * steps_max * NX * 32;
+  T* const REC0 = scr;
+  T* BL = REC0 + cs_off + (long long)args.ns_max * NX * C * 32;
   T* BR = BL + 2 * rm * NX;
+  const int phases = FWD_ONLY ? 1 : (args.phases ? args.phases : 3);
 
   const double alpha = 1.4426950408889634 / fmax(2.0 * args.param * args.param, 1e-12);
   const bool rbf = RBF_NOPAR || args.kind == KIND_RBF;
@@ -133,6 +143,11 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
   for (long long tid = wg; tid < args.ntasks; tid += nw) {
     const int2 ab = decode_task((int)tid, args.mode, args.nY, args.list, args.order);
     const int task = args.order ? args.order[tid] : (int)tid;
+    T* REC = args.rec ? args.rec + (long long)task * args.rec_per_pair : REC0;
+    T* CS = REC + cs_off;
+    if constexpr (FWD_ONLY) {
+      if (lane == 0) args.lev[task] = 1.0;  // level 0; levels >= 1 start at 0
+    }
     if (ab.x < 0 || ab.x >= args.nX || ab.y < 0 || ab.y >= args.nYseq) {
       if (lane == 0) set_status(args.status, KSIG_ERR_INVALID);
       continue;
@@ -149,7 +164,8 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
     T w[NL + 1];
 #pragma unroll
     for (int k = 0; k <= NL; ++k)
-      w[k] = (k >= 1 && k <= args.nl_out) ? (T)args.glev[(long long)k * args.ntasks + task] : T(0);
+      w[k] = (!FWD_ONLY && k >= 1 && k <= args.nl_out)
+                 ? (T)args.glev[(long long)k * args.ntasks + task] : T(0);
 
     const T* xb = args.xr + args.xstart[a] * RS;
     const T* yb = args.yr + args.ystart[b] * RS;
@@ -187,9 +203,13 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
     auto rec_at = [&](int s, long long t) { return REC + ((long long)s * steps_max + t) * NX * 32; };
 
     T Ccol[NX][C];  // forward column sums (rows above the current row)
+    // Forward-only launches: per-lane level totals (FP64), levels 1..NL.
+    double lt[NL + 1];
+#pragma unroll
+    for (int k = 0; k <= NL; ++k) lt[k] = 0.0;
 
     // ---------------- phase 1: forward, top-down, strips left to right -----
-    for (int s = 0; s < ns; ++s) {
+    for (int s = 0; s < ((phases & 1) ? ns : 0); ++s) {
       stage_y(s);
 #pragma unroll
       for (int h = 0; h < NX; ++h)
@@ -244,6 +264,7 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
 #pragma unroll
         for (int h = 0; h < NX; ++h) H[h] = Xin[h];
         if (P == 1) {
+          T top = T(0);  // forward-only: this row's level-NL terms
 #pragma unroll
           for (int c = 0; c < C; ++c) {
             const T z = Z[c];
@@ -256,7 +277,9 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
             if (NL >= 2) Ccol[0][c] += z;
 #pragma unroll
             for (int k = 2; k < NL; ++k) Ccol[k - 1][c] = fma(z, Hold[k - 2], Ccol[k - 1][c]);
+            if constexpr (FWD_ONLY && NL >= 2) top = fma(z, Hold[NL - 2], top);
           }
+          if constexpr (FWD_ONLY) lt[NL] += (double)top;
         } else {
 #pragma unroll
           for (int c = 0; c < C; ++c) {
@@ -321,7 +344,19 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
 #pragma unroll
         for (int k = 0; k < RS; ++k) xc[k] = xn[k];
       }
-      if (ns > 1 && s + 1 < ns) {
+      if constexpr (FWD_ONLY) {
+        // Level k < NL of this strip: the sum of its final column sums.
+#pragma unroll
+        for (int k = 1; k < NL; ++k) {
+          double sk = 0.0;
+#pragma unroll
+          for (int c = 0; c < C; ++c) sk += (double)Ccol[k - 1][c];
+          lt[k] += sk;
+        }
+      }
+      // Final column sums: read back by the adjoint pass (the last strip's
+      // stay in registers when both passes run in one launch).
+      if ((ns > 1 && s + 1 < ns) || !(phases & 2)) {
         T* dst = CS + (long long)s * NX * C * 32;
 #pragma unroll
         for (int h = 0; h < NX; ++h)
@@ -330,11 +365,21 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
       }
       __syncwarp();  // carries and records of this strip -> later readers
     }
+    if constexpr (FWD_ONLY) {
+      // Level totals of the pair: lanes summed in a fixed order (FP64).
+#pragma unroll
+      for (int k = 1; k <= NL; ++k) {
+        double v = lt[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+        if (lane == 0 && k <= args.nl_out) args.lev[(long long)k * args.ntasks + task] = v;
+      }
+    }
 
     // ---------------- phase 2: adjoint, bottom-up, strips right to left ----
-    for (int s = ns - 1; s >= 0; --s) {
+    for (int s = (phases & 2) ? ns - 1 : -1; s >= 0; --s) {
       stage_y(s);
-      if (s != ns - 1) {
+      if (s != ns - 1 || !(phases & 1)) {
         const T* src = CS + (long long)s * NX * C * 32;
 #pragma unroll
         for (int h = 0; h < NX; ++h)
@@ -704,9 +749,22 @@ template <typename T, int KD, int C, int NL, int P, int WPB>
 __global__ void __launch_bounds__(WPB * 32)
 dp_bwd_kernel(const DpBwdArgs<T> args) {
   if (args.kind == KIND_RBF && args.dparam == nullptr)
-    dp_bwd_body<T, KD, C, NL, P, WPB, true>(args);
+    dp_bwd_body<T, KD, C, NL, P, WPB, true, false>(args);
   else
-    dp_bwd_body<T, KD, C, NL, P, WPB, false>(args);
+    dp_bwd_body<T, KD, C, NL, P, WPB, false, false>(args);
+}
+
+// Forward pass of the split gradient pass (order 1): phase 1 with per-pair
+// records and level totals, in a kernel of its own so that the adjoint
+// kernel's register allocation is not shared with it.
+template <typename T, int KD, int C, int NL, int P, int WPB>
+__global__ void __launch_bounds__(WPB * 32)
+dp_rec_fwd_kernel(const DpBwdArgs<T> args) {
+  static_assert(P == 1, "the split gradient pass is order 1");
+  if (args.kind == KIND_RBF)
+    dp_bwd_body<T, KD, C, NL, P, WPB, true, true>(args);
+  else
+    dp_bwd_body<T, KD, C, NL, P, WPB, false, true>(args);
 }
 
 }  // namespace ksig

@@ -14,6 +14,7 @@ enum KernelOp : int {
   OP_DP_FWD_EXT = 4,   // dp_fwd_kernel, EXT: the other static kernels
   OP_PDE_FWD_EXT = 5,  // pde_fwd_kernel, EXT
   OP_GA_FWD = 6,       // SweepArgs<T>      ga_fwd_kernel (global alignment)
+  OP_DP_REC_FWD = 7,   // DpBwdArgs<T>      dp_rec_fwd_kernel (split gradient pass)
 };
 
 struct KernelEntry {

@@ -213,6 +213,11 @@ class SignatureBase:
     raise NotImplementedError(
         f'gradients are not available for {type(self).__name__}')
 
+  def _split_pass(self):
+    """(forward, adjoint) of the split gradient pass for K(X, Y), or None
+    where it does not apply."""
+    return None
+
   def _K_autograd(self, Xin, Xs, gx, Ys, gy, sym):
     """Differentiable K(X, Y) / K(X) through the hand-written adjoint."""
     kind, param = self._static()
@@ -222,7 +227,7 @@ class SignatureBase:
     pt = self._param_tensor()
     spec = dict(Xs=Xs, Ys=Ys, normalize=self.normalize, kind=kind,
                 param=float(param), levels_fn=self._levels,
-                bwd_fn=self._levels_bwd,
+                bwd_fn=self._levels_bwd, rec_fn=self._split_pass(),
                 param_dtype=pt.dtype if pt is not None else torch.float64,
                 param_device=pt.device if pt is not None else 'cpu',
                 const_level0=not isinstance(self, SignaturePDEKernel))
@@ -253,6 +258,23 @@ class SignatureKernel(SignatureBase):
     kind, param = self._static()
     return E.sig_levels_bwd(Xs, Ys, mode, self.n_levels, self.order, kind,
                             param, grad_levels, want_dparam=want_dparam)
+
+  def _split_pass(self):
+    """Order 1 with differencing: the autograd forward runs the forward
+    pass of the adjoint kernel and keeps its per-pair records (when they fit
+    the memory budget of ``_engine.rec_budget_bytes``), so the backward runs
+    only the adjoint pass."""
+    if self.order != 1 or self.n_levels < 2 or not self.difference:
+      return None
+    kind, param = self._static()
+
+    def fwd(Xs, Ys):
+      return E.sig_levels_rec(Xs, Ys, self.n_levels, 1, kind, param)
+
+    def bwd(Xs, Ys, grad_levels, want_dparam, ws):
+      return E.sig_levels_bwd_rec(Xs, Ys, self.n_levels, 1, kind, param,
+                                  grad_levels, ws, want_dparam=want_dparam)
+    return fwd, bwd
 
   def _Kdiag(self, Xs):
     """ksig/kernels.py:166-178: ones when normalising."""
@@ -308,6 +330,9 @@ class SignaturePDEKernel(SignatureKernel):
     kind, param = self._static()
     return E.pde_values_bwd(Xs, Ys, mode, self.dyadic_order, kind, param,
                             grad_levels[0], want_dparam=want_dparam)
+
+  def _split_pass(self):
+    return None  # the split gradient pass is the DP adjoint's
 
 
 class GlobalAlignmentKernel(SignatureBase):

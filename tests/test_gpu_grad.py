@@ -174,3 +174,62 @@ def test_dp_grad_deep_truncation(dt, tol):
        lambda x, y, b: OT.signature_kernel(x, y, n_levels=10, order=1,
                                            normalize=True, param=b),
        X, Y, 0.9, dt, tol)
+
+
+@pytest.mark.parametrize('dt,tol', [(torch.float64, 1e-10), (torch.float32, 2e-6)])
+@pytest.mark.parametrize('L,ragged', [(40, False), (260, False), (150, True)])
+@pytest.mark.parametrize('kind', ['rbf', 'linear'])
+def test_split_gradient_pass_matches_one_launch(dt, tol, L, ragged, kind):
+  """ksig_signature_kern_rec_fwd / _rec_bwd (forward pass with per-pair
+  records, then the adjoint pass alone) against ksig_signature_kern and
+  ksig_signature_kern_bwd: levels, dX and dparam, single- and multi-strip
+  (260 columns), ragged lengths."""
+  from ksig_b200 import _engine as E, _lib as Lb
+  rng = np.random.default_rng(L + 7 * ragged)
+  X = torch.tensor(_walks(rng, 3, L, 4), dtype=dt, device='cuda')
+  Y = torch.tensor(_walks(rng, 4, L + 13, 4), dtype=dt, device='cuda')
+  lx = ly = None
+  if ragged:
+    lx = torch.tensor([L, L // 2, 7], dtype=torch.int32, device='cuda')
+    ly = torch.tensor([L + 13, 3, L // 3, 1], dtype=torch.int32, device='cuda')
+  Xs, Ys = E.Seqs(X, lx), E.Seqs(Y, ly)
+  k = Lb.STATIC_RBF if kind == 'rbf' else Lb.STATIC_LINEAR
+  par = 0.9 if kind == 'rbf' else 0.7
+  m = 5
+  ref = E.sig_levels(Xs, Ys, Lb.PAIRS_FULL, m, 1, True, k, par)
+  out = E.sig_levels_rec(Xs, Ys, m, 1, k, par)
+  assert out is not None
+  lev, ws = out
+  assert _relerr(lev, ref) < tol
+  gl = torch.tensor(np.random.default_rng(3).standard_normal(tuple(ref.shape)),
+                    device='cuda')
+  dX0, dp0 = E.sig_levels_bwd(Xs, Ys, Lb.PAIRS_FULL, m, 1, k, par, gl)
+  dX1, dp1 = E.sig_levels_bwd_rec(Xs, Ys, m, 1, k, par, gl, ws)
+  assert _relerr(dX1, dX0) < tol
+  assert abs(dp1.item() - dp0.item()) <= tol * max(1.0, abs(dp0.item()))
+
+
+@pytest.mark.parametrize('dt,tol', [(torch.float64, 1e-10), (torch.float32, 2e-6)])
+def test_split_gradient_pass_through_autograd(dt, tol, monkeypatch):
+  """K(X, Y) gradients with the split pass (default) and without it
+  (KSIG_REC_MB=0), normalised, X and Y and the bandwidth requiring grad."""
+  import ksig_b200 as K
+  rng = np.random.default_rng(11)
+  X = _walks(rng, 3, 70, 3)
+  Y = _walks(rng, 2, 90, 3)
+
+  def run():
+    Xt = torch.tensor(X, dtype=dt, device='cuda', requires_grad=True)
+    Yt = torch.tensor(Y, dtype=dt, device='cuda', requires_grad=True)
+    bt = torch.tensor(0.8, dtype=torch.float64, requires_grad=True)
+    kern = K.SignatureKernel(n_levels=4, order=1, static_kernel=K.RBFKernel(bt))
+    out = kern(Xt, Yt)
+    W = torch.tensor(np.random.default_rng(5).standard_normal(tuple(out.shape)),
+                     device='cuda', dtype=out.dtype)
+    (out * W).sum().backward()
+    return out.detach(), Xt.grad, Yt.grad, bt.grad
+  a = run()
+  monkeypatch.setenv('KSIG_REC_MB', '0')
+  b = run()
+  for u, v in zip(a, b):
+    assert _relerr(u, v) < tol
