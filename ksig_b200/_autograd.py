@@ -50,18 +50,25 @@ class SigKernelFn(torch.autograd.Function):
     lev_fn = spec['levels_fn']
     sym = Ys is None
     out_dtype = Xs.data.dtype
+    split = spec.get('rec_fn')
+    use_split = split is not None and (Xt is not None or pt is not None)
     if sym:
-      lev = lev_fn(Xs, None, L.PAIRS_UPPER)
+      # The backward differentiates all ordered pairs; with the split pass
+      # the forward records them all and keeps the upper triangle.
+      rec = split[0](Xs, Xs) if use_split else None
+      if rec is not None:
+        levf, ctx.rec_ws = rec
+        a, b = _upper_index(Xs.n, levf.device)
+        lev = levf[:, a * Xs.n + b].contiguous()
+      else:
+        lev = lev_fn(Xs, None, L.PAIRS_UPPER)
       K = E.normalize_levels(lev, L.PAIRS_UPPER, Xs.n, Xs.n, None, None,
                              spec['normalize'], out_dtype)
       dx = dy = None
     else:
       # Split gradient pass: the forward keeps the adjoint's records, the
       # backward replays them (see SignatureKernel._split_pass).
-      rec = None
-      split = spec.get('rec_fn')
-      if split is not None and (Xt is not None or pt is not None):
-        rec = split[0](Xs, Ys)
+      rec = split[0](Xs, Ys) if use_split else None
       if rec is not None:
         lev, ctx.rec_ws = rec
       else:
@@ -119,7 +126,11 @@ class SigKernelFn(torch.autograd.Function):
         gK[:, idx, idx] += gKx + gKy
       W = gK + gK.transpose(1, 2)  # diagonal counted twice: both sides
       if want_x or want_p:
-        dXd, dp = bwd(Xs, Xs, L.PAIRS_FULL, W.reshape(n_lev, -1), want_p)
+        if ctx.rec_ws is not None:
+          dXd, dp = spec['rec_fn'][1](Xs, Xs, W.reshape(n_lev, -1), want_p,
+                                      ctx.rec_ws)
+        else:
+          dXd, dp = bwd(Xs, Xs, L.PAIRS_FULL, W.reshape(n_lev, -1), want_p)
         dX = dXd if want_x else None
         if dp is not None:
           dpar_total += 0.5 * dp

@@ -210,9 +210,11 @@ def test_split_gradient_pass_matches_one_launch(dt, tol, L, ragged, kind):
 
 
 @pytest.mark.parametrize('dt,tol', [(torch.float64, 1e-10), (torch.float32, 2e-6)])
-def test_split_gradient_pass_through_autograd(dt, tol, monkeypatch):
-  """K(X, Y) gradients with the split pass (default) and without it
-  (KSIG_REC_MB=0), normalised, X and Y and the bandwidth requiring grad."""
+@pytest.mark.parametrize('sym', [False, True])
+def test_split_gradient_pass_through_autograd(dt, tol, sym, monkeypatch):
+  """K(X, Y) and K(X) gradients with the split pass (default) and without
+  it (KSIG_REC_MB=0), normalised, the inputs and the bandwidth requiring
+  grad."""
   import ksig_b200 as K
   rng = np.random.default_rng(11)
   X = _walks(rng, 3, 70, 3)
@@ -223,11 +225,12 @@ def test_split_gradient_pass_through_autograd(dt, tol, monkeypatch):
     Yt = torch.tensor(Y, dtype=dt, device='cuda', requires_grad=True)
     bt = torch.tensor(0.8, dtype=torch.float64, requires_grad=True)
     kern = K.SignatureKernel(n_levels=4, order=1, static_kernel=K.RBFKernel(bt))
-    out = kern(Xt, Yt)
+    out = kern(Xt) if sym else kern(Xt, Yt)
     W = torch.tensor(np.random.default_rng(5).standard_normal(tuple(out.shape)),
                      device='cuda', dtype=out.dtype)
     (out * W).sum().backward()
-    return out.detach(), Xt.grad, Yt.grad, bt.grad
+    gy = torch.zeros(1) if sym else Yt.grad
+    return out.detach(), Xt.grad, gy, bt.grad
   a = run()
   monkeypatch.setenv('KSIG_REC_MB', '0')
   b = run()
