@@ -160,7 +160,9 @@ class SigKernelFn(torch.autograd.Function):
             dY = dYd2 if dY is None else dY + dYd2
           if dp is not None:
             dpar_total += 0.5 * dp
-    ctx.rec_ws = None  # the records are used once
+    if ctx.rec_ws is not None:  # the records are used once
+      E.rec_release(ctx.rec_ws)
+      ctx.rec_ws = None
     gx = gy = None
     if want_x and dX is not None and ctx.x_meta is not None:
       shape, dtype, device = ctx.x_meta

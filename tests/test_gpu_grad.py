@@ -236,3 +236,22 @@ def test_split_gradient_pass_through_autograd(dt, tol, sym, monkeypatch):
   b = run()
   for u, v in zip(a, b):
     assert _relerr(u, v) < tol
+
+
+def test_split_pass_workspace_reused():
+  """The backward hands the split pass's workspace back and the next
+  forward takes the same buffer (no new allocation per step)."""
+  import ksig_b200 as K
+  from ksig_b200 import _engine as E
+  rng = np.random.default_rng(12)
+  X = torch.tensor(_walks(rng, 3, 60, 3), dtype=torch.float32, device='cuda',
+                   requires_grad=True)
+  Y = torch.tensor(_walks(rng, 2, 50, 3), dtype=torch.float32, device='cuda')
+  kern = K.SignatureKernel(n_levels=4, order=1, static_kernel=K.RBFKernel(0.8))
+  E.rec_pool_clear()
+  ptrs = []
+  for _ in range(3):
+    kern(X, Y).sum().backward()
+    ptrs.append(E._REC_POOL[torch.cuda.current_device()].data_ptr())
+  assert ptrs[0] == ptrs[1] == ptrs[2]
+  E.rec_pool_clear()
