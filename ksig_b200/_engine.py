@@ -189,11 +189,12 @@ def sig_levels_bwd(X, Y, mode, n_levels, order, kind, param, grad_levels,
   return dX, dpar
 
 
-# Split-pass workspaces (tens of GB) handed back by the backward are kept,
-# one per device, for the next forward: going through torch's cache instead,
-# smaller tensors split the freed block and every step paid a new cudaMalloc
-# of the whole workspace.  Calls on one stream are ordered, so the next
-# forward's kernels run after the backward that released the buffer.
+# Split-pass workspaces (up to tens of GB) handed back by the backward are
+# kept per device for the next forwards: going through torch's cache
+# instead, smaller tensors split the freed blocks and steps paid a new
+# cudaMalloc of the whole workspace.  Calls on one stream are ordered, so a
+# forward's kernels run after the backward that released its buffer.  The
+# pool holds at most KSIG_REC_MB bytes per device.
 _REC_POOL = {}
 
 
@@ -201,22 +202,35 @@ def _dev_index(device):
   return device.index if device.index is not None else torch.cuda.current_device()
 
 
+def _rec_cap():
+  return int(os.environ.get('KSIG_REC_MB', '65536')) << 20
+
+
 def rec_budget_bytes(device):
   """Memory the split gradient pass may keep for its records:
   ``KSIG_REC_MB`` (default 65536), at most half of the free device memory
-  (a pooled workspace counts as available)."""
-  cap = int(os.environ.get('KSIG_REC_MB', '65536')) << 20
+  (the largest pooled workspace counts as available)."""
   free, _ = torch.cuda.mem_get_info(device)
-  pooled = _REC_POOL.get(_dev_index(device))
-  return min(cap, free // 2 + (pooled.numel() if pooled is not None else 0))
+  pool = _REC_POOL.get(_dev_index(device), [])
+  return min(_rec_cap(), free // 2 + max((w.numel() for w in pool), default=0))
+
+
+def _rec_take(nbytes, device):
+  """The smallest pooled workspace of at least ``nbytes``, else a new one."""
+  pool = _REC_POOL.setdefault(_dev_index(device), [])
+  fit = [i for i, w in enumerate(pool) if w.numel() >= nbytes]
+  if fit:
+    return pool.pop(min(fit, key=lambda i: pool[i].numel()))
+  return _workspace(nbytes, device)
 
 
 def rec_release(ws):
   """Hands a split-pass workspace back for reuse by the next forward."""
-  idx = _dev_index(ws.device)
-  old = _REC_POOL.get(idx)
-  if old is None or old.numel() <= ws.numel():
-    _REC_POOL[idx] = ws
+  pool = _REC_POOL.setdefault(_dev_index(ws.device), [])
+  pool.append(ws)
+  pool.sort(key=lambda w: -w.numel())
+  while sum(w.numel() for w in pool) > _rec_cap():
+    pool.pop()  # the smallest goes back to torch
 
 
 def rec_pool_clear():
@@ -240,11 +254,7 @@ def sig_levels_rec(X, Y, n_levels, order, kind, param, pair_list=None):
   P = num_pairs(mode, X.n, Y.n, n_list)
   out = torch.empty((n_levels + 1, max(P, 0)), dtype=torch.float64,
                     device=X.data.device)
-  idx = _dev_index(X.data.device)
-  ws = _REC_POOL.pop(idx, None)
-  if ws is None or ws.numel() < ws_bytes:
-    ws = None  # too small: released before the larger allocation
-    ws = _workspace(ws_bytes, X.data.device)
+  ws = _rec_take(ws_bytes, X.data.device)
   rc = lib.ksig_signature_kern_rec_fwd(
       _ptr(X.data), _ptr(X.lengths), X.n, X.L, _ptr(Y.data), _ptr(Y.lengths),
       Y.n, Y.L, X.d, dt, kind, float(param), n_levels, order, 1, mode,

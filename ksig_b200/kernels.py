@@ -185,7 +185,8 @@ class SignatureBase:
       Ys, _, gy = _to_seqs(Y, self.n_features)
     if diag:
       K = self._Kdiag(Xs)
-    elif gx is not None or gy is not None or self._param_requires_grad():
+    elif torch.is_grad_enabled() and (gx is not None or gy is not None or
+                                      self._param_requires_grad()):
       K = self._K_autograd(X if gx is not None else None, Xs, gx,
                            Ys, gy, Y is None)
     else:

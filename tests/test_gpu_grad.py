@@ -252,6 +252,8 @@ def test_split_pass_workspace_reused():
   ptrs = []
   for _ in range(3):
     kern(X, Y).sum().backward()
-    ptrs.append(E._REC_POOL[torch.cuda.current_device()].data_ptr())
+    pool = E._REC_POOL[torch.cuda.current_device()]
+    assert len(pool) == 1
+    ptrs.append(pool[0].data_ptr())
   assert ptrs[0] == ptrs[1] == ptrs[2]
   E.rec_pool_clear()
