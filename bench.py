@@ -334,6 +334,7 @@ def run_ours(args, rank, world, dist):
   # Forward + backward (gradient of sum(W * K) w.r.t. X through the adjoint
   # kernels), the 'fwd+bwd s/step' half of the metric.
   fb_ms = None
+  split_used = None
   if not args.no_bwd:
     Xg = Xd.clone().requires_grad_(True)
     Wt = torch.randn((N_SEQ, N_SEQ), device=dev, dtype=torch.float32)
@@ -358,6 +359,9 @@ def run_ours(args, rank, world, dist):
       b.synchronize()
       fbs.append(a.elapsed_time(b))
     fb_ms = sum(fbs) / len(fbs)
+    # Whether the split gradient pass ran (its workspace is pooled after a
+    # backward) rather than the sweep plus the one-launch adjoint.
+    split_used = bool(E._REC_POOL.get(torch.cuda.current_device()))
     if dist is not None:
       t = torch.tensor([fb_ms], device=dev, dtype=torch.float64)
       dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -409,7 +413,8 @@ def run_ours(args, rank, world, dist):
         'fwd_bwd': None if fb_ms is None else {
             's_per_step': fb_ms * 1e-3, 'ms_per_step': fb_ms,
             'what': 'K(X, Y) forward + dL/dX backward (L = sum W*K), '
-                    'X [512, 200, 9] requires grad', 'steps': args.bwd_steps},
+                    'X [512, 200, 9] requires grad', 'steps': args.bwd_steps,
+            'split_pass': split_used},
         'gpu_launches': int(launches),
         'clocks': clk,
         'cpu_baseline': cpu,

@@ -208,11 +208,14 @@ def _rec_cap():
 
 def rec_budget_bytes(device):
   """Memory the split gradient pass may keep for its records:
-  ``KSIG_REC_MB`` (default 65536), at most half of the free device memory
-  (the largest pooled workspace counts as available)."""
+  ``KSIG_REC_MB`` (default 65536), at most half of the available device
+  memory: free memory plus what torch's cache holds unused (the largest
+  pooled workspace counts as available too)."""
   free, _ = torch.cuda.mem_get_info(device)
+  cached = torch.cuda.memory_reserved(device) - torch.cuda.memory_allocated(device)
   pool = _REC_POOL.get(_dev_index(device), [])
-  return min(_rec_cap(), free // 2 + max((w.numel() for w in pool), default=0))
+  return min(_rec_cap(),
+             (free + max(cached, 0)) // 2 + max((w.numel() for w in pool), default=0))
 
 
 def _rec_take(nbytes, device):
