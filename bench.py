@@ -377,6 +377,12 @@ def run_ours(args, rank, world, dist):
                      '(oracle/ksig_oracle.py), single process',
            'seconds': secs}
 
+  # The large ragged order-2 workload (one GPU): forward and forward +
+  # input gradient, fused vs plain on a sample, errors against the oracle.
+  ragged = None
+  if world == 1 and not args.no_ragged:
+    ragged = ragged_record(args)
+
   entries = N_SEQ * N_SEQ * world
   if rank == 0:
     line = {
@@ -384,11 +390,16 @@ def run_ours(args, rank, world, dist):
         'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
         'ms_per_step': t_step, 'higher_is_better': True, 'scaling': 'weak',
         'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
-        'config': config(world, {'l2': 'flushed (256 MB write) between steps'}),
+        'config': config(world),
+        'l2': 'flushed (256 MB write) between timed steps',
         'roofline': {'bound': 'fp32', 'achieved': achieved,
                      'peak': peak.value, 'unit': 'TFLOP/s',
                      'frac': achieved / peak.value if peak.value else None,
                      'traffic': traffic,
+                     'traffic_source': 'dram__bytes_read.sum + dram__bytes_write.sum of '
+                                       'one ncu capture of this launch, committed as '
+                                       'profiles/dp_fwd_traffic.json (not measured in '
+                                       'this run)' if traffic else None,
                      'kernel': 'dp_fwd_kernel (512x512 pair sweep)',
                      'kernel_ms': k_ms,
                      'peak_source': 'measured live: FP32 FMA-chain probe '
@@ -418,6 +429,7 @@ def run_ours(args, rank, world, dist):
         'gpu_launches': int(launches),
         'clocks': clk,
         'cpu_baseline': cpu,
+        'ragged_dp': ragged,
     }
     print(json.dumps(line))
 
@@ -442,17 +454,59 @@ def make_ragged(n, lmin, lmax, d, seed):
           for L in lens]
 
 
-def run_ragged(args):
+def _sample_errors(kern, R, Xl, Yl, dev):
+  """Per-entry errors on the sample whose FP64 oracle values are committed
+  in tests/golden/ragged_dp_sample.npz (written by make_ragged_sample.py
+  from the same seeded batch): the normalised K of 4 x 4 pairs holding the
+  longest sequences of each side, and dL/dX of 2 x 2 of them."""
+  import torch
+  path = os.path.join(ROOT, 'tests', 'golden', 'ragged_dp_sample.npz')
+  if not os.path.exists(path):
+    return None
+  f = np.load(path)
+  Xs = [Xl[i] for i in f['ix']]
+  Ys = [Yl[i] for i in f['iy']]
+  K = kern(Xs, Ys, return_on_gpu=True).double().cpu().numpy()
+  ref = f['K']
+  k_err = float(np.max(np.abs(K - ref) / np.abs(ref)))
+  Xg = [Xl[i].clone().requires_grad_(True) for i in f['gx']]
+  Yg = [Yl[i] for i in f['gy']]
+  W = torch.tensor(f['W'], device=dev, dtype=torch.float32)
+  (kern(Xg, Yg, return_on_gpu=True) * W).sum().backward()
+  g_err = 0.0
+  for j, x in enumerate(Xg):
+    g = x.grad.double().cpu().numpy()
+    r = f['dX'][j, :g.shape[0]]
+    floor = 1e-2 * np.max(np.abs(r))
+    g_err = max(g_err, float(np.max(np.abs(g - r) / np.maximum(np.abs(r), floor))))
+  return {'pairs': int(len(Xs) * len(Ys)),
+          'lengths_x': [int(Xl[i].shape[0]) for i in f['ix']],
+          'lengths_y': [int(Yl[i].shape[0]) for i in f['iy']],
+          'max_rel_err_K': k_err,
+          'max_rel_err_dX': g_err,
+          'dX_pairs': int(len(Xg) * len(Yg)),
+          'bar': 'K: |err| / |ref| per entry (target 1e-5); dX: |err| / '
+                 'max(|ref|, 1e-2 max|ref|) per coordinate (target 1e-4)',
+          'reference': 'FP64 oracle (oracle/ksig_oracle.py, autograd through '
+                       'oracle/ksig_oracle_torch.py) on the FP32-rounded inputs, '
+                       'committed as tests/golden/ragged_dp_sample.npz'}
+
+
+def ragged_record(args, fwd_steps=1, bwd_steps=1):
+  """Times the ragged order-2 workload through the public API (lists of
+  device tensors): forward, and forward + input gradient; the fused and plain
+  kernels on a bounded sample of the same pairs; and the per-entry errors of
+  the oracle sample."""
   import torch
 
   import ksig_b200 as K
   from ksig_b200 import _engine as E
   from ksig_b200 import _lib as Lb
   R = dict(RAGGED)
-  if args.n_seq is not None:
+  if args.n_seq is not None and args.workload == 'ragged-dp':
     R['n'] = args.n_seq
   n, m, p, bw = R['n'], R['n_levels'], R['order'], R['bw']
-  dev = torch.device('cuda', 0)
+  dev = torch.device('cuda', torch.cuda.current_device())
   Xl = [torch.as_tensor(a, device=dev) for a in make_ragged(n, R['lmin'], R['lmax'], R['d'], 5)]
   Yl = [torch.as_tensor(a, device=dev) for a in make_ragged(n, R['lmin'], R['lmax'], R['d'], 6)]
   lx = np.array([a.shape[0] for a in Xl])
@@ -477,14 +531,14 @@ def run_ragged(args):
       ts.append(a.elapsed_time(b))
     return sum(ts) / len(ts)
 
-  fwd_ms = timed(lambda: kern(Xl, Yl, return_on_gpu=True), args.steps, 1)
+  fwd_ms = timed(lambda: kern(Xl, Yl, return_on_gpu=True), fwd_steps, 1)
   Xg = [a.clone().requires_grad_(True) for a in Xl]
 
   def fb():
     Kg = kern(Xg, Yl, return_on_gpu=True)
     (Kg * W).sum().backward()
 
-  fb_ms = timed(fb, args.bwd_steps, 1)
+  fb_ms = timed(fb, bwd_steps, 0)
 
   # Fused vs plain kernels on the same bounded sample of pairs.
   s = min(args.plain_sample, n)
@@ -501,33 +555,36 @@ def run_ragged(args):
   f_fwd = timed(lambda: E.sig_levels(Xs, Ys, Lb.PAIRS_FULL, m, p, True, Lb.STATIC_RBF, bw), 2, 1)
   f_bwd = timed(lambda: E.sig_levels_bwd(Xs, Ys, Lb.PAIRS_FULL, m, p, Lb.STATIC_RBF, bw, gl,
                                          want_dparam=False), 2, 1)
-  p_fwd = timed(lambda: E.sig_levels_plain(Xs, Ys, Lb.PAIRS_FULL, m, p, Lb.STATIC_RBF, bw), 1, 1)
+  p_fwd = timed(lambda: E.sig_levels_plain(Xs, Ys, Lb.PAIRS_FULL, m, p, Lb.STATIC_RBF, bw), 1, 0)
   p_bwd = timed(lambda: E.sig_levels_bwd_plain(Xs, Ys, Lb.PAIRS_FULL, m, p, Lb.STATIC_RBF, bw,
-                                               gl, want_dparam=False), 1, 1)
-  # FP32 levels against the FP64 path (pinned to the oracle) on a corner.
-  c = min(16, s)
-  Xc, Yc = seqs(Xl[:c]), seqs(Yl[:c])
-  l32 = E.sig_levels(Xc, Yc, Lb.PAIRS_FULL, m, p, True, Lb.STATIC_RBF, bw)
-  l64 = E.sig_levels(E.Seqs(Xc.data.double(), Xc.lengths), E.Seqs(Yc.data.double(), Yc.lengths),
-                     Lb.PAIRS_FULL, m, p, True, Lb.STATIC_RBF, bw)
-  scale = l64.abs().amax(dim=1, keepdim=True).clamp_min(1e-300)
-  rel = float(((l32 - l64).abs() / scale).max())
-  line = {
-      'metric': METRIC, 'workload': f'sig_dp_rbf_ragged_N{n}_M{n}_L32-1024_d16_m{m}_p{p}_normalized',
-      'forward': {'value': n * n / (fwd_ms * 1e-3), 'unit': UNIT, 'ms_per_step': fwd_ms,
-                  'cells_per_s': cells / (fwd_ms * 1e-3)},
-      'fwd_bwd': {'s_per_step': fb_ms * 1e-3,
-                  'what': 'K(X, Y) + d sum(W*K)/dX through the public API (ragged lists)'},
-      'sample': {'pairs': s * s, 'cells': scells,
-                 'fused_fwd_ms': f_fwd, 'fused_bwd_ms': f_bwd,
-                 'plain_fwd_ms': p_fwd, 'plain_bwd_ms': p_bwd,
-                 'speedup_fwd': p_fwd / f_fwd, 'speedup_bwd': p_bwd / f_bwd,
-                 'speedup_fwd_bwd': (p_fwd + p_bwd) / (f_fwd + f_bwd),
-                 'plain_fwd_bwd_full_s_est': (p_fwd + p_bwd) * 1e-3 * cells / scells},
-      'rel_err_fp32_vs_fp64_levels': rel,
-      'cells': cells, 'steps': args.steps, 'bwd_steps': args.bwd_steps,
-      'dtype': 'f32', 'data': 'synthetic',
+                                               gl, want_dparam=False), 1, 0)
+  errs = _sample_errors(kern, R, Xl, Yl, dev) if n == RAGGED['n'] else None
+  return {
+      'workload': f'sig_dp_rbf_ragged_N{n}_M{n}_L32-1024_d16_m{m}_p{p}_normalized',
+      'forward': {'value': n * n / (fwd_ms * 1e-3), 'unit': UNIT, 's_per_step': fwd_ms * 1e-3,
+                  'cells_per_s': cells / (fwd_ms * 1e-3), 'steps': fwd_steps},
+      'fwd_bwd': {'s_per_step': fb_ms * 1e-3, 'steps': bwd_steps,
+                  'what': 'K(X, Y) + d sum(W*K)/dX through the public API (ragged lists '
+                          'of device tensors)'},
+      'plain_vs_fused_sample': {
+          'pairs': s * s, 'cells': scells,
+          'what': f'the first {s} x {s} pairs: plain FP32 one-pair-per-block kernels '
+                  '(ksig_signature_kern_plain / _plain_bwd) against the fused '
+                  'forward and adjoint kernels on the same levels',
+          'fused_fwd_ms': f_fwd, 'fused_bwd_ms': f_bwd,
+          'plain_fwd_ms': p_fwd, 'plain_bwd_ms': p_bwd,
+          'speedup_fwd': p_fwd / f_fwd, 'speedup_bwd': p_bwd / f_bwd,
+          'speedup_fwd_bwd': (p_fwd + p_bwd) / (f_fwd + f_bwd),
+          'plain_fwd_bwd_full_s_est': (p_fwd + p_bwd) * 1e-3 * cells / scells,
+          'speedup_fwd_bwd_full_est': (p_fwd + p_bwd) * 1e-3 * cells / scells / (fb_ms * 1e-3)},
+      'oracle_sample': errs,
+      'cells': cells, 'dtype': 'f32', 'data': 'synthetic (seeded, bench.make_ragged)',
   }
+
+
+def run_ragged(args):
+  line = {'metric': METRIC}
+  line.update(ragged_record(args, args.steps, args.bwd_steps))
   print(json.dumps(line))
 
 
@@ -711,6 +768,15 @@ def run_mmd_pde(args):
 # Reference arm: the reference recursion on the host cores.
 # ---------------------------------------------------------------------------
 
+def _cupy_probe():
+  """Whether the reference's own GPU path (CuPy) could run on this host."""
+  try:
+    import cupy  # noqa: F401
+    return {'available': True, 'version': getattr(cupy, '__version__', '?')}
+  except Exception as e:  # noqa: BLE001 - any import failure means unavailable
+    return {'available': False, 'reason': f'{type(e).__name__}: {e}'[:200]}
+
+
 def run_reference(args, rank, world):
   if rank != 0:
     return
@@ -739,6 +805,9 @@ def run_reference(args, rank, world):
                                  f'{cores}-process pool'},
       'e2e': {'value': value, 'unit': UNIT, 'h2d_bytes_per_step': 0,
               'd2h_bytes_per_step': 0},
+      # The reference's CuPy path on the GPU needs CuPy, which this image
+      # does not ship; the probe records why it is not timed.
+      'reference_cupy_path': _cupy_probe(),
   }
   print(json.dumps(line))
 
@@ -754,6 +823,8 @@ def main():
   ap.add_argument('--no-cpu', action='store_true')
   ap.add_argument('--no-bwd', action='store_true')
   ap.add_argument('--no-plain', action='store_true')
+  ap.add_argument('--no-ragged', action='store_true',
+                  help='skip the ragged order-2 sub-record of the bench line')
   ap.add_argument('--bwd-steps', type=int, default=5)
   ap.add_argument('--workload', default='dp512',
                   choices=['dp512', 'ragged-dp', 'ragged-pde', 'mmd-pde'],

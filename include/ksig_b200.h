@@ -120,13 +120,18 @@ int ksig_signature_kern(const void* X, const int32_t* lenX, int nX, int LX,
  * owns the device memory, a loop that cannot take cudaMalloc's device-wide
  * synchronisation).  Its scratch is a 16 MiB array compiled into the
  * library: every GPU that loads the library holds it until the process
- * exits.  Calls whose ksig_signature_kern_workspace(...) exceeds 16 MiB are
- * rejected with KSIG_ERR_WORKSPACE.  It calls no cudaMalloc / cudaFree.
- * The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture.  All calls share the array and keep the last
- * call's contents (each call clears what must start at zero), so calls
- * that overlap on the GPU race: order them on one stream or synchronise.
+ * exits.  Tasks run in their natural order (no longest-first order buffers),
+ * so a call needs the workspace of that unordered plan, which is at most
+ * ksig_signature_kern_workspace(...); calls whose unordered plan exceeds
+ * 16 MiB are rejected with KSIG_ERR_WORKSPACE.  It calls no cudaMalloc /
+ * cudaFree.  Every call looks up the array's device address
+ * (cudaGetSymbolAddress) with the call's device current; the first lookup
+ * on a device loads the library's device code there, so make the first call
+ * on each device before any stream capture.  All calls share the array and
+ * keep the last call's contents (each call clears what must start at zero),
+ * so calls that overlap on the GPU race: order them on one stream or
+ * synchronise.  Lengths outside [1, L] are clamped and flagged in the
+ * array's status word; ksig_static_status reads it.
  */
 int ksig_signature_kern_static(const void* X, const int32_t* lenX, int nX,
                                int LX, const void* Y, const int32_t* lenY,
@@ -367,6 +372,13 @@ int ksig_normalize_levels(const double* levels, int n_lev, int pairs_mode,
  * KSIG_ERR_DEVICE.  No reference counterpart (CuPy raises on the host).
  */
 int ksig_workspace_status(void* workspace, void* stream);
+
+/*
+ * ksig_workspace_status for the scratch array of ksig_signature_kern_static
+ * on the current device (whose address callers cannot see).  Like that
+ * entry point, it has no counterpart in the reference.
+ */
+int ksig_static_status(void* stream);
 
 /*
  * Measurement helpers (no reference counterpart).

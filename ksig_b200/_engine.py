@@ -192,9 +192,11 @@ def sig_levels_bwd(X, Y, mode, n_levels, order, kind, param, grad_levels,
 # Split-pass workspaces (up to tens of GB) handed back by the backward are
 # kept per device for the next forwards: going through torch's cache
 # instead, smaller tensors split the freed blocks and steps paid a new
-# cudaMalloc of the whole workspace.  Calls on one stream are ordered, so a
-# forward's kernels run after the backward that released its buffer.  The
-# pool holds at most KSIG_REC_MB bytes per device.
+# cudaMalloc of the whole workspace.  A released buffer carries an event
+# recorded on the releasing stream after the backward's kernels; the stream
+# that takes it waits on that event first, so a forward on another stream
+# cannot overwrite records the adjoint is still reading.  The pool holds at
+# most KSIG_REC_MB bytes per device.
 _REC_POOL = {}
 
 
@@ -223,13 +225,20 @@ def _rec_take(nbytes, device):
   pool = _REC_POOL.setdefault(_dev_index(device), [])
   fit = [i for i, w in enumerate(pool) if w.numel() >= nbytes]
   if fit:
-    return pool.pop(min(fit, key=lambda i: pool[i].numel()))
+    ws = pool.pop(min(fit, key=lambda i: pool[i].numel()))
+    ev = getattr(ws, '_ksig_released', None)
+    if ev is not None:
+      torch.cuda.current_stream(ws.device).wait_event(ev)
+    return ws
   return _workspace(nbytes, device)
 
 
 def rec_release(ws):
   """Hands a split-pass workspace back for reuse by the next forward."""
   pool = _REC_POOL.setdefault(_dev_index(ws.device), [])
+  ev = torch.cuda.Event()
+  ev.record(torch.cuda.current_stream(ws.device))
+  ws._ksig_released = ev
   pool.append(ws)
   pool.sort(key=lambda w: -w.numel())
   while sum(w.numel() for w in pool) > _rec_cap():

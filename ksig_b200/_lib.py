@@ -56,6 +56,7 @@ _SIGNATURES = {
     'ksig_normalize_levels': (_I, [_P, _I, _I, _I, _I, _P, _P, _I, _P, _I,
                                    _P]),
     'ksig_workspace_status': (_I, [_P, _P]),
+    'ksig_static_status': (_I, [_P]),
     'ksig_signature_kern_bwd_workspace': (_SZ, [_I] * 11),
     'ksig_signature_kern_bwd': (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _I, _I,
                                      _I, _D, _I, _I, _I, _I, _P, _I, _P, _P,

@@ -129,6 +129,40 @@ def instances():
     for p, nls in ((3, [3, 4, 5, 6, 8]), (4, [4, 5, 6, 8])):
       for nl, kd in itertools.product(nls, KD_FEW):
         add(('dpb', dt, kd, 2, nl, p, 1))
+  # Orders 5 to 8 (order 0 = full order up to n_levels 8), forward and
+  # adjoint: the narrowest tile only (the level states grow as p^2).
+  for dt in ('f32', 'f64'):
+    for p in (5, 6, 7, 8):
+      for nl, kd in itertools.product([nl for nl in (5, 6, 8) if nl >= p], KD_FEW):
+        add(('dp', dt, kd, 2, nl, p, 1))
+        add(('dpb', dt, kd, 2, nl, p, 1))
+  # Deeper truncations: order 1 up to 32 levels, order 2 up to 16.
+  for dt in ('f32', 'f64'):
+    for (p, nl), kd in itertools.product(
+        [(1, 16), (1, 20), (1, 24), (1, 32), (2, 10), (2, 12), (2, 16)], KD_FEW):
+      add(('dp', dt, kd, 2, nl, p, 1))
+      add(('dpb', dt, kd, 2, nl, p, 1))
+  # Gram-input forward sweeps (kd = 0, gram.cuh): every channel count and
+  # static kind, for the shapes the register-Gram tiles do not cover.
+  for dt in ('f32', 'f64'):
+    wide = [2, 4, 7] if dt == 'f32' else [2]
+    for nl, c in itertools.product(NL_ALL + [10, 12, 16, 20, 24, 32], wide):
+      add(('dp', dt, 0, c, nl, 1, 1))
+    for nl, c in itertools.product([2, 3, 4, 5, 6, 8, 10, 12, 16], wide[:2]):
+      add(('dp', dt, 0, c, nl, 2, 1))
+    for p in (3, 4, 5, 6, 7, 8):
+      for nl in (3, 4, 5, 6, 8):
+        if nl >= p:
+          add(('dp', dt, 0, 2, nl, p, 1))
+    for p, nls in ((1, NL_ALL), (2, [2, 3, 4, 5, 6, 8])):
+      for nl in nls:
+        add(('dp', dt, 0, 2, nl, p, 0))
+    for f, c in itertools.product([1, 2, 4, 8], [2, 4, 8] if dt == 'f32' else [2]):
+      add(('pde', dt, 0, c, 0, f, 1))
+    for f in (1, 2, 4):
+      add(('pde', dt, 0, 2, 0, f, 0))
+    for c in ([2, 4, 8] if dt == 'f32' else [2]):
+      add(('ga', dt, 0, c, 0, 1, 0))
   # Forward pass of the split gradient pass: one per order-1 adjoint tile
   # with at least two levels (same tile, same records).
   out += [('dpr',) + inst[1:] for inst in out
@@ -148,6 +182,11 @@ OPS = {
 }
 
 
+HEADER = {'dp': 'sweep.cuh', 'pde': 'sweep.cuh', 'dpx': 'sweep.cuh',
+          'pdex': 'sweep.cuh', 'ga': 'sweep.cuh', 'dpb': 'dp_bwd.cuh',
+          'dpr': 'dp_bwd.cuh', 'pdeb': 'pde_bwd.cuh'}
+
+
 def _group_key(inst):
   op, dt, kd, c, nl, p, diff = inst
   return f'{op}_{dt}_p{p}_d{diff}_kd{kd}'
@@ -162,9 +201,10 @@ def generate():
   units = []
   tables = []
   for key, insts in sorted(groups.items()):
+    # Each unit includes only the header of its kernel family, so that an
+    # edit to one family's header rebuilds only that family.
     lines = ['// Generated by ksig_b200/build.py; do not edit.',
-             '#include "../sweep.cuh"', '#include "../dp_bwd.cuh"',
-             '#include "../pde_bwd.cuh"',
+             f'#include "../{HEADER[insts[0][0]]}"',
              '#include "../registry.h"',
              'namespace ksig {']
     ents = []
@@ -210,11 +250,30 @@ def _write_if_changed(path, text):
     f.write(text)
 
 
-def _headers():
-  hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC)
-        if f.endswith(('.cuh', '.h'))]
-  hs.append(os.path.join(ROOT, 'include', 'ksig_b200.h'))
-  return hs
+_INC_CACHE = {}
+
+
+def _includes(path):
+  """Files a source includes with #include "...", transitively."""
+  path = os.path.normpath(path)
+  if path in _INC_CACHE:
+    return _INC_CACHE[path]
+  _INC_CACHE[path] = set()
+  out = set()
+  try:
+    with open(path) as f:
+      text = f.read()
+  except OSError:
+    return out
+  for line in text.splitlines():
+    line = line.strip()
+    if line.startswith('#include "'):
+      inc = os.path.normpath(os.path.join(os.path.dirname(path), line.split('"')[1]))
+      if os.path.exists(inc):
+        out.add(inc)
+        out |= _includes(inc)
+  _INC_CACHE[path] = out
+  return out
 
 
 def _nvcc():
@@ -223,7 +282,7 @@ def _nvcc():
 
 
 def _compile(src, obj, force):
-  deps = [src] + _headers() + [os.path.abspath(__file__)]
+  deps = [src] + sorted(_includes(src)) + [os.path.abspath(__file__)]
   if (not force and os.path.exists(obj)
       and os.path.getmtime(obj) >= max(os.path.getmtime(d) for d in deps)):
     return obj, None

@@ -18,6 +18,7 @@
 #include "dp_bwd.cuh"
 #include "pde_bwd.cuh"
 #include "plain.cuh"
+#include "gram.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
 
@@ -154,6 +155,12 @@ const KernelEntry* find_kernel(int op, int f64, int need_kd, int want_c, int nee
 
 size_t align_up(size_t v, size_t a = 256) { return (v + a - 1) / a * a; }
 
+// RBF exponent scale a = log2(e) / max(2 s^2, 1e-12) (ksig/static/kernels.py:
+// 258-260 in base 2); 0 for the other kinds.
+double rbf_alpha(int kind, double param) {
+  return kind == KSIG_STATIC_RBF ? 1.4426950408889634 / fmax(2.0 * param * param, 1e-12) : 0.0;
+}
+
 // Workspace carve-up shared by the forward kernels.
 struct FwdPlan {
   int f64, kd, rs, c, nl, nl_out, p, diff, nx_exchange;
@@ -163,8 +170,12 @@ struct FwdPlan {
   long long rows_max, scratch_per_warp, nwarps;
   int ordered;            // workspace holds a longest-first task order
   size_t sort_tmp;        // radix-sort temporary bytes
+  // Gram input (gram.cuh): the call runs in chunks of gram_chunk tasks, each
+  // with a [gram_rows][gram_ld] slot of static-kernel values.
+  int gin, gram_rows, gram_ld;
+  long long gram_chunk, gram_slot;
   size_t off_status, off_xr, off_yr, off_xstart, off_ystart, off_xlen, off_ylen,
-      off_okeys, off_okeys2, off_ovals, off_order, off_sort, off_scratch, total;
+      off_okeys, off_okeys2, off_ovals, off_order, off_sort, off_scratch, off_gram, total;
   const KernelEntry* k;
 };
 
@@ -188,6 +199,8 @@ void layout_fwd(FwdPlan& pl, int nX, int LX, int nY, int LY) {
   pl.off_order = off; off = align_up(off + no);
   pl.off_sort = off; off = align_up(off + (pl.ordered ? pl.sort_tmp : 0));
   pl.off_scratch = off; off = align_up(off + (size_t)pl.nwarps * pl.scratch_per_warp * es);
+  pl.off_gram = off;
+  if (pl.gin) off = align_up(off + (size_t)pl.gram_chunk * pl.gram_slot * es);
   pl.total = off;
 }
 
@@ -318,9 +331,12 @@ int want_cols(int ly_cells, int cap, int op) {
 
 // family: 0 DP, 1 PDE (order_or_dyadic = dyadic order), 2 global alignment
 // (no differencing; order_or_dyadic unused).
+// layout_only: the packing and workspace layout without a sweep kernel (the
+// plain one-pair-per-block kernels use it; any d, order and n_levels).
 int plan_fwd(int family, int nX, int LX, int nY, int LY, int d, int dtype, int n_levels,
              int order_or_dyadic, int difference, int pairs_mode, int n_list,
-             FwdPlan& pl, bool allow_order = true, bool ext = false) {
+             FwdPlan& pl, bool allow_order = true, bool ext = false,
+             bool layout_only = false) {
   const bool pde = family == 1, ga = family == 2;
   if (dtype != KSIG_DTYPE_F32 && dtype != KSIG_DTYPE_F64)
     return fail(KSIG_ERR_INVALID, "dtype must be KSIG_DTYPE_F32 or KSIG_DTYPE_F64");
@@ -355,7 +371,32 @@ int plan_fwd(int family, int nX, int LX, int nY, int LY, int d, int dtype, int n
   const int op = ga ? OP_GA_FWD
                    : ext ? (pde ? OP_PDE_FWD_EXT : OP_DP_FWD_EXT) : (pde ? OP_PDE_FWD : OP_DP_FWD);
   const int want = want_cols(ly_cells, 8, op);
-  const KernelEntry* k = find_kernel(op, pl.f64, d, want, need_nl, p, pl.diff);
+  const KernelEntry* k = layout_only ? nullptr : find_kernel(op, pl.f64, d, want, need_nl, p, pl.diff);
+  if (layout_only) {
+    pl.k = nullptr;
+    pl.kd = round_up(d, 4);
+    pl.c = 1;
+    pl.nl = need_nl;
+    pl.nl_out = need_nl;
+    pl.p = p;
+    pl.wpb = 1;
+    pl.rs = round_up(pl.kd + 1, pl.f64 ? 2 : 4);
+    pl.grid = 1;
+    pl.nwarps = 0;
+    pl.scratch_per_warp = 0;
+    if (allow_order) plan_order(pl, pairs_mode);
+    layout_fwd(pl, nX, LX, nY, LY);
+    return KSIG_OK;
+  }
+  if (!k) {
+    // No register-Gram tile for this shape (e.g. more channels than the
+    // widest compiled one): the Gram-input instantiation of the same family
+    // with a precomputed Gram (any static kind, any d).
+    const int gop = ga ? OP_GA_FWD : (pde ? OP_PDE_FWD : OP_DP_FWD);
+    k = find_kernel(gop, pl.f64, 0, want, need_nl, p, pl.diff);
+    if (k && k->kd != 0) k = nullptr;
+    if (k) pl.gin = 1;
+  }
   if (!k)
     return fail(KSIG_ERR_UNSUPPORTED,
                 "no compiled %s kernel for dtype=%s d=%d n_levels=%d order/F=%d difference=%d%s",
@@ -363,7 +404,7 @@ int plan_fwd(int family, int nX, int LX, int nY, int LY, int d, int dtype, int n
                 p, pl.diff,
                 ext ? " (polynomial / Matern / rational quadratic static kernel)" : "");
   pl.k = k;
-  pl.kd = k->kd;
+  pl.kd = pl.gin ? round_up(d, 4) : k->kd;
   pl.c = k->c;
   pl.nl = k->nl;
   pl.nl_out = need_nl;
@@ -383,7 +424,7 @@ int plan_fwd(int family, int nX, int LX, int nY, int LY, int d, int dtype, int n
     pl.nx_exchange = nh > 0 ? nh : 1;
   }
   // Grid: one warp per SM slot, never more warps than pairs.
-  pl.dyn_smem = sweep_dyn_smem_bytes(k->wpb, pl.c, pl.rs, es);
+  pl.dyn_smem = sweep_dyn_smem_bytes(k->wpb, pl.c, pl.gin ? 1 : pl.rs, es);
   cudaError_t e = ensure_smem_attr(k->func, pl.dyn_smem);
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(MaxDynamicSharedMemorySize)");
   int occ = 0;
@@ -397,6 +438,17 @@ int plan_fwd(int family, int nX, int LX, int nY, int LY, int d, int dtype, int n
   pl.rows_max = lx_cells > 32 ? lx_cells : 32;
   pl.scratch_per_warp = pl.multi ? pl.rows_max * pl.nx_exchange : 0;
   pl.nwarps = nwarps;
+  if (pl.gin) {
+    pl.gram_rows = LX;
+    pl.gram_ld = LY;
+    pl.gram_slot = (long long)LX * LY;
+    const long long budget = (long long)env_int("KSIG_GRAM_MB", 4096) << 20;
+    long long chunk = budget / (pl.gram_slot * (long long)es);
+    if (chunk < 1) chunk = 1;
+    if (chunk > np) chunk = np > 0 ? np : 1;
+    if (chunk > 65535) chunk = 65535;  // grid.y of gram_kernel
+    pl.gram_chunk = chunk;
+  }
   if (allow_order) plan_order(pl, pairs_mode);
   layout_fwd(pl, nX, LX, nY, LY);
   return KSIG_OK;
@@ -459,8 +511,11 @@ int run_fwd(const FwdPlan& pl, const void* X, const int32_t* lenX, int nX, int L
                         &rc);
   if (rc) return rc;
   a.ntasks = (int)pl.ntasks;
+  a.ntasks_total = (int)pl.ntasks;
+  a.task_base = 0;
   a.kind = kind;
   a.sp = sp;
+  a.ralpha = (T)rbf_alpha(kind, param);
   a.out = out;
   a.scratch = pl.multi ? reinterpret_cast<T*>(ws + pl.off_scratch) : nullptr;
   a.scratch_per_warp = pl.scratch_per_warp;
@@ -470,7 +525,34 @@ int run_fwd(const FwdPlan& pl, const void* X, const int32_t* lenX, int nX, int L
   a.nYseq = self ? nX : nY;
   a.status = status;
   void* kargs[] = {&a};
-  KSIG_CUDA(launch_main(pl.k->func, dim3(pl.grid), dim3(pl.k->wpb * 32), kargs, pl.dyn_smem, st));
+  if (!pl.gin) {
+    KSIG_CUDA(launch_main(pl.k->func, dim3(pl.grid), dim3(pl.k->wpb * 32), kargs, pl.dyn_smem, st));
+    return KSIG_OK;
+  }
+  // Gram input: per chunk of tasks, the Gram slots, then the sweep on them.
+  GramArgs<T> g{};
+  g.xr = xr; g.xstart = xs; g.xlen = xl; g.yr = yr; g.ystart = ys; g.ylen = yl;
+  g.rs = pl.rs; g.kd = pl.kd;
+  g.mode = mode; g.nY = a.nY; g.list = a.list; g.order = a.order;
+  g.nX = nX; g.nYseq = a.nYseq;
+  g.kind = kind; g.ralpha = a.ralpha; g.sp = sp;
+  g.gram = reinterpret_cast<T*>(ws + pl.off_gram);
+  g.slot = pl.gram_slot; g.ld = pl.gram_ld;
+  const int tiles_x = (pl.gram_rows + kGramTile - 1) / kGramTile;
+  g.tiles_y = (pl.gram_ld + kGramTile - 1) / kGramTile;
+  g.status = status;
+  a.gram = g.gram; a.gram_slot = pl.gram_slot; a.gram_ld = pl.gram_ld;
+  for (long long t0 = 0; t0 < pl.ntasks; t0 += pl.gram_chunk) {
+    const long long nt = pl.ntasks - t0 < pl.gram_chunk ? pl.ntasks - t0 : pl.gram_chunk;
+    g.task_base = (int)t0; g.ntasks = (int)nt;
+    gram_kernel<T><<<dim3(tiles_x * g.tiles_y, (unsigned)nt), 256, 0, st>>>(g);
+    KSIG_CUDA(cudaGetLastError());
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    a.task_base = (int)t0; a.ntasks = (int)nt;
+    const long long blocks = (nt + pl.k->wpb - 1) / pl.k->wpb;
+    const int grid = blocks < pl.grid ? (int)blocks : pl.grid;
+    KSIG_CUDA(launch_main(pl.k->func, dim3(grid), dim3(pl.k->wpb * 32), kargs, pl.dyn_smem, st));
+  }
   return KSIG_OK;
 }
 
@@ -750,11 +832,10 @@ struct PlainPlan {
 int plan_plain(int nX, int LX, int nY, int LY, int d, int dtype, int n_levels, int order,
                int pairs_mode, int n_list, PlainPlan& pp) {
   int rc = plan_fwd(false, nX, LX, nY, LY, d, dtype, n_levels, order, 1, pairs_mode, n_list,
-                    pp.f);
+                    pp.f, false, false, true);
   if (rc) return rc;
   if (pairs_mode == KSIG_PAIRS_UPPER || pairs_mode == KSIG_PAIRS_DIAG) { nY = nX; LY = LX; }
   pp.order = pp.f.p;
-  if (pp.order > 4) return fail(KSIG_ERR_UNSUPPORTED, "plain baseline supports order <= 4");
   const long long lx = LX > 1 ? LX - 1 : 1, ly = LY > 1 ? LY - 1 : 1;
   pp.cap = lx * ly;
   const size_t es = pp.f.f64 ? 8 : 4;
@@ -797,6 +878,7 @@ int run_plain(const PlainPlan& pp, const void* X, const int32_t* lenX, int nX, i
   a.list = reinterpret_cast<const int2*>(list);
   a.ntasks = (int)pl.ntasks; a.nX = nX; a.nYseq = self ? nX : nY;
   a.kind = kind; a.n_levels = n_levels; a.order = pp.order;
+  a.ralpha = (T)rbf_alpha(kind, param);
   a.out = out;
   a.scratch = reinterpret_cast<T*>(ws + pp.off_scratch);
   a.cap = pp.cap;
@@ -867,6 +949,7 @@ int run_plain_bwd(const PlainBwdPlan& bp, const void* X, const int32_t* lenX, in
   f.list = reinterpret_cast<const int2*>(list);
   f.ntasks = (int)pl.ntasks; f.nX = nX; f.nYseq = self ? nX : nY;
   f.kind = kind; f.n_levels = n_levels; f.order = pp.order;
+  f.ralpha = (T)rbf_alpha(kind, param);
   f.out = nullptr;
   f.scratch = reinterpret_cast<T*>(ws + pp.off_scratch);
   f.cap = pp.cap;
@@ -936,6 +1019,31 @@ int check_common(const void* X, const void* Y, int pairs_mode, const int32_t* li
   return KSIG_OK;
 }
 
+// The plain one-pair-per-block DP kernel as the generic path for shapes no
+// fused instantiation covers (orders above 8, more than 32 levels): any d,
+// order and n_levels, same outputs.
+int plain_entry(const void* X, const int32_t* lenX, int nX, int LX, const void* Y,
+                const int32_t* lenY, int nY, int LY, int d, int dtype, int static_kind,
+                double static_param, int n_levels, int order, int pairs_mode,
+                const int32_t* list, int n_list, double* out, void* ws, size_t ws_bytes,
+                void* stream) {
+  PlainPlan pp;
+  int rc = plan_plain(nX, LX, nY, LY, d, dtype, n_levels, order, pairs_mode, n_list, pp);
+  if (rc) return rc;
+  if (!ws || ws_bytes < pp.total)
+    return fail(KSIG_ERR_WORKSPACE, "workspace of %zu bytes is smaller than the %zu required",
+                ws_bytes, pp.total);
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  KSIG_CUDA(cudaMemsetAsync(ws, 0, 16, st));
+  if (pp.f.ntasks == 0) return KSIG_OK;
+  if (pairs_mode == KSIG_PAIRS_UPPER || pairs_mode == KSIG_PAIRS_DIAG) { nY = nX; LY = LX; Y = X; lenY = lenX; }
+  if (dtype == KSIG_DTYPE_F64)
+    return run_plain<double>(pp, X, lenX, nX, LX, Y, lenY, nY, LY, d, 1, static_kind, static_param,
+                             n_levels, pairs_mode, list, out, static_cast<char*>(ws), st);
+  return run_plain<float>(pp, X, lenX, nX, LX, Y, lenY, nY, LY, d, 0, static_kind, static_param,
+                          n_levels, pairs_mode, list, out, static_cast<char*>(ws), st);
+}
+
 int fwd_entry(int family, const void* X, const int32_t* lenX, int nX, int LX, const void* Y,
               const int32_t* lenY, int nY, int LY, int d, int dtype, int static_kind,
               double static_param, int n_levels, int order_or_dyadic, int difference,
@@ -959,6 +1067,10 @@ int fwd_entry(int family, const void* X, const int32_t* lenX, int nX, int LX, co
   const bool ext = static_kind != KSIG_STATIC_RBF && static_kind != KSIG_STATIC_LINEAR;
   rc = plan_fwd(family, nX, LX, nY, LY, d, dtype, n_levels, order_or_dyadic, difference,
                 pairs_mode, n_list, pl, allow_order, ext);
+  if (rc == KSIG_ERR_UNSUPPORTED && family == 0 && !ext && difference)
+    return plain_entry(X, lenX, nX, LX, Y, lenY, nY, LY, d, dtype, static_kind, static_param,
+                       n_levels, order_or_dyadic, pairs_mode, list, n_list, out, ws, ws_bytes,
+                       stream);
   if (rc) return rc;
   if (!ws || ws_bytes < pl.total)
     return fail(KSIG_ERR_WORKSPACE, "workspace of %zu bytes is smaller than the %zu required",
@@ -1004,30 +1116,16 @@ __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 
 // Device address of g_static_scratch on the current device.  In host code
 // the symbol's name is only a host-side stand-in, never a device address,
-// so it is resolved with cudaGetSymbolAddress once per device, with that
-// device current, and cached.
+// so it is resolved with cudaGetSymbolAddress, with the device current.  It
+// is looked up on every call (cheap once the module is loaded), so the
+// address stays right after a cudaDeviceReset reloads the module; the first
+// lookup on a device loads the module, which is why the first call of
+// ksig_signature_kern_static on a device should come before any stream
+// capture.
 void* static_scratch_ptr(cudaError_t* err) {
-  static std::mutex mu;
-  static std::vector<void*> ptrs;
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) {
-    *err = e;
-    return nullptr;
-  }
-  std::lock_guard<std::mutex> lk(mu);
-  if ((int)ptrs.size() <= dev) ptrs.resize(dev + 1, nullptr);
-  if (!ptrs[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_static_scratch);
-    if (e != cudaSuccess) {
-      *err = e;
-      return nullptr;
-    }
-    ptrs[dev] = p;
-  }
-  *err = cudaSuccess;
-  return ptrs[dev];
+  void* p = nullptr;
+  *err = cudaGetSymbolAddress(&p, g_static_scratch);
+  return *err == cudaSuccess ? p : nullptr;
 }
 
 }  // namespace
@@ -1056,9 +1154,15 @@ size_t ksig_signature_kern_workspace(int nX, int LX, int nY, int LY, int d, int 
                                      int n_levels, int order, int difference, int pairs_mode,
                                      int n_list) {
   FwdPlan pl;
-  if (plan_fwd(false, nX, LX, nY, LY, d, dtype, n_levels, order, difference, pairs_mode, n_list,
-               pl))
+  if (int rc = plan_fwd(false, nX, LX, nY, LY, d, dtype, n_levels, order, difference, pairs_mode,
+                        n_list, pl)) {
+    // No fused instantiation: the plain kernel's workspace (fwd_entry).
+    PlainPlan pp;
+    if (rc == KSIG_ERR_UNSUPPORTED && difference &&
+        !plan_plain(nX, LX, nY, LY, d, dtype, n_levels, order, pairs_mode, n_list, pp))
+      return pp.total;
     return 0;
+  }
   // Also large enough for the other static kernels' instantiations
   // (ksig_signature_kern_ex), where one is compiled for this shape.
   FwdPlan px;
@@ -1249,8 +1353,15 @@ size_t ksig_signature_kern_bwd_workspace(int nX, int LX, int nY, int LY, int d, 
                                          int n_levels, int order, int difference,
                                          int pairs_mode, int n_list) {
   BwdPlan bp;
-  if (plan_bwd(nX, LX, nY, LY, d, dtype, n_levels, order, difference, pairs_mode, n_list, bp))
+  if (int rc = plan_bwd(nX, LX, nY, LY, d, dtype, n_levels, order, difference, pairs_mode,
+                        n_list, bp)) {
+    // No fused adjoint for this shape: the plain adjoint's workspace.
+    PlainBwdPlan pb;
+    if (rc == KSIG_ERR_UNSUPPORTED && difference &&
+        !plan_plain_bwd(nX, LX, nY, LY, d, dtype, n_levels, order, pairs_mode, n_list, pb))
+      return pb.pp.total;
     return 0;
+  }
   return bp.total;
 }
 
@@ -1265,6 +1376,13 @@ int ksig_signature_kern_bwd(const void* X, const int32_t* lenX, int nX, int LX, 
   if (!grad_levels || !dX) return fail(KSIG_ERR_INVALID, "grad_levels / dX is NULL");
   BwdPlan bp;
   rc = plan_bwd(nX, LX, nY, LY, d, dtype, n_levels, order, difference, pairs_mode, n_list, bp);
+  if (rc == KSIG_ERR_UNSUPPORTED && difference)
+    // Shapes no fused adjoint covers (d above 32, orders above 8, more than
+    // 32 levels): the plain one-pair-per-block adjoint, same results.
+    return ksig_signature_kern_plain_bwd(X, lenX, nX, LX, Y, lenY, nY, LY, d, dtype, static_kind,
+                                         static_param, n_levels, order, pairs_mode, pair_list,
+                                         n_list, grad_levels, dX, dparam, workspace,
+                                         workspace_bytes, stream);
   if (rc) return rc;
   if (!workspace || workspace_bytes < bp.total)
     return fail(KSIG_ERR_WORKSPACE, "workspace of %zu bytes is smaller than the %zu required",
@@ -1498,6 +1616,13 @@ int ksig_fp32_peak(double* tflops, void* stream) {
   const double flops = 2.0 * 8.0 * (double)iters * blocks * threads;
   *tflops = flops / (best * 1e-3) / 1e12;
   return KSIG_OK;
+}
+
+int ksig_static_status(void* stream) {
+  cudaError_t e = cudaSuccess;
+  void* ws = static_scratch_ptr(&e);
+  if (!ws) return cuda_fail(e, "cudaGetSymbolAddress(g_static_scratch)");
+  return ksig_workspace_status(ws, stream);
 }
 
 int ksig_workspace_status(void* workspace, void* stream) {

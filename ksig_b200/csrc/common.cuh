@@ -87,6 +87,139 @@ __device__ __forceinline__ double packed_arg(const XA& x, const YA& y, double) {
   return acc;
 }
 
+// ---- RBF arguments in a lane-centred frame --------------------------------
+// RBF rows are packed raw (x itself, norm slot zero).  A lane that owns the
+// grid columns y_0 .. y_{C-1} of a strip (plus, in the adjoints, the next
+// lane's first column y_C) moves the origin to its own first point c = y_0:
+//   column slot 0:      -c                       (norm slot 0)
+//   column slot c >= 1: (2a (y_c - c), -a |y_c - c|^2)
+// and a grid row x becomes x' = x - c with norm slot -a |x'|^2, so that
+//   arg_0 = -a |x'|^2,   arg_c = x'[KD] + y_c[KD] + sum_k x'_k y_c[k]
+// (centred_arg on the transformed rows) is -a |x - y_c|^2 with a =
+// log2(e) / max(2 s^2, 1e-12) (ksig/static/kernels.py:258-260).  The columns
+// of one lane lie within a few steps of c, so |y_c - c| is small; then
+// |x'|^2 + |y'|^2 - 2 <x', y'> cannot cancel (|x'| near |y'| means both are
+// small), unlike |x|^2 + |y|^2 - 2 <x, y> for long unnormalised paths, where
+// both norms reach 1e4 in FP32.  Column 0 needs no dot product at all.
+
+// Raw column points y[c][0..KD] (slot KD zero) -> lane-centred form; slot 0
+// is the centre.  NC columns in a [NC][KD + 1] array.
+template <int KD, int NC, typename T>
+__device__ __forceinline__ void rbf_center_cols(T (&y)[NC][KD + 1], T alpha) {
+  const T two_a = T(2) * alpha;
+#pragma unroll
+  for (int c = 1; c < NC; ++c) {
+    T n = T(0);
+#pragma unroll
+    for (int k = 0; k < KD; ++k) {
+      const T v = y[c][k] - y[0][k];
+      n = fma(v, v, n);
+      y[c][k] = two_a * v;
+    }
+    y[c][KD] = -alpha * n;
+  }
+#pragma unroll
+  for (int k = 0; k < KD; ++k) y[0][k] = -y[0][k];
+  y[0][KD] = T(0);
+}
+
+// One column of the lane-centred form from its raw point and the raw centre
+// (for column storage outside a register array).
+template <int KD, typename YA, typename CA, typename T>
+__device__ __forceinline__ void rbf_center_col(YA& y, const CA& c0, T alpha) {
+  const T two_a = T(2) * alpha;
+  T n = T(0);
+#pragma unroll
+  for (int k = 0; k < KD; ++k) {
+    const T v = y[k] - c0[k];
+    n = fma(v, v, n);
+    y[k] = two_a * v;
+  }
+  y[KD] = -alpha * n;
+}
+
+// Grid row x (raw) -> x' = x + negc (negc = column slot 0) with the norm
+// slot -a |x'|^2; xt may alias x.  FP32 pairs coordinates (FADD2 / FFMA2).
+template <int KD, typename XA, typename NA>
+__device__ __forceinline__ void rbf_center_row(const XA& x, const NA& negc, float alpha,
+                                               float* xt) {
+  if constexpr (KD >= 4) {
+    float2 n2 = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int j = 0; j < KD / 2; ++j) {
+      const float2 v = __fadd2_rn(make_float2(x[2 * j], x[2 * j + 1]),
+                                  make_float2(negc[2 * j], negc[2 * j + 1]));
+      xt[2 * j] = v.x;
+      xt[2 * j + 1] = v.y;
+      n2 = __ffma2_rn(v, v, n2);
+    }
+    float n = n2.x + n2.y;
+    if constexpr (KD % 2 == 1) {
+      const float v = x[KD - 1] + negc[KD - 1];
+      xt[KD - 1] = v;
+      n = fmaf(v, v, n);
+    }
+    xt[KD] = -alpha * n;
+  } else {
+    float n = 0.f;
+#pragma unroll
+    for (int k = 0; k < KD; ++k) {
+      const float v = x[k] + negc[k];
+      xt[k] = v;
+      n = fmaf(v, v, n);
+    }
+    xt[KD] = -alpha * n;
+  }
+}
+template <int KD, typename XA, typename NA>
+__device__ __forceinline__ void rbf_center_row(const XA& x, const NA& negc, double alpha,
+                                               double* xt) {
+  double n = 0.0;
+#pragma unroll
+  for (int k = 0; k < KD; ++k) {
+    const double v = x[k] + negc[k];
+    xt[k] = v;
+    n = fma(v, v, n);
+  }
+  xt[KD] = -alpha * n;
+}
+
+// RBF argument of a centred row x' (rbf_center_row) and a centred column y
+// (rbf_center_cols): y[KD] + sum_k x'_k y_k + xnorm, with the row's norm
+// term xnorm = x'[KD] added last, so that the dot-product chains do not
+// wait for the norm chain of the same row.  PAIR as in packed_arg.
+template <int KD, bool PAIR, typename XA, typename YA>
+__device__ __forceinline__ float centred_arg(const XA& x, const YA& y, float xnorm) {
+  if constexpr (PAIR && KD >= 5) {
+    float2 s;
+    if constexpr (KD % 2 == 1) {
+      s = make_float2(y[KD], x[KD - 1] * y[KD - 1]);
+#pragma unroll
+      for (int j = 0; j < KD / 2; ++j)
+        s = __ffma2_rn(make_float2(x[2 * j], x[2 * j + 1]), make_float2(y[2 * j], y[2 * j + 1]), s);
+      return (s.x + s.y) + xnorm;
+    } else {
+      s = make_float2(y[KD], 0.f);
+#pragma unroll
+      for (int j = 0; j < KD / 2; ++j)
+        s = __ffma2_rn(make_float2(x[2 * j], x[2 * j + 1]), make_float2(y[2 * j], y[2 * j + 1]), s);
+      return (s.x + s.y) + xnorm;
+    }
+  } else {
+    float acc = y[KD];
+#pragma unroll
+    for (int k = 0; k < KD; ++k) acc = fmaf(x[k], y[k], acc);
+    return acc + xnorm;
+  }
+}
+template <int KD, bool PAIR, typename XA, typename YA>
+__device__ __forceinline__ double centred_arg(const XA& x, const YA& y, double xnorm) {
+  double acc = y[KD];
+#pragma unroll
+  for (int k = 0; k < KD; ++k) acc = fma(x[k], y[k], acc);
+  return acc + xnorm;
+}
+
 // Static kernel value from the fused dot-product argument (RBF, linear).
 template <typename T>
 __device__ __forceinline__ T static_value(T arg, int kind) {

@@ -135,9 +135,11 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
   const double alpha = 1.4426950408889634 / fmax(2.0 * args.param * args.param, 1e-12);
   const bool rbf = RBF_NOPAR || args.kind == KIND_RBF;
   const bool want_dpar = !RBF_NOPAR && args.dparam != nullptr;
-  const T inv2a = T(1.0 / (2.0 * alpha));
+  const T ralpha = T(alpha);
+  // dM/dx = M (y - x) / s^2 (RBF; the row sums below carry 2a (y - x)) or
+  // s y (linear).
   const double xscale = rbf ? 1.0 / (args.param * args.param) : args.param;
-  const T xscale_t = T(xscale);
+  const T xscale_t = T(rbf ? xscale / (2.0 * alpha) : xscale);
   double dpar_w = 0.0;
 
   for (long long tid = wg; tid < args.ntasks; tid += nw) {
@@ -170,15 +172,34 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
     const T* xb = args.xr + args.xstart[a] * RS;
     const T* yb = args.yr + args.ystart[b] * RS;
     // Column points of strip s (C own columns + the next lane's first).
+    // RBF: stored in the lane-centred frame of rbf_center_cols (slot 0 the
+    // negated centre, slots 1..C relative to it).
     auto stage_y = [&](int s) {
+      const int col0 = s * STRIP + C * lane;
+      T c0[RS];
+      {
+        const V* p = reinterpret_cast<const V*>(yb + (long long)(col0 < Ly - 1 ? col0 : Ly - 1) * RS);
 #pragma unroll
-      for (int c = 0; c <= C; ++c) {
-        int col = s * STRIP + C * lane + c;
+        for (int v = 0; v < RV; ++v) reinterpret_cast<V*>(c0)[v] = __ldg(p + v);
+      }
+#pragma unroll
+      for (int c = 1; c <= C; ++c) {
+        int col = col0 + c;
         col = col < Ly - 1 ? col : Ly - 1;
         const V* p = reinterpret_cast<const V*>(yb + (long long)col * RS);
+        T yv[RS];
 #pragma unroll
-        for (int v = 0; v < RV; ++v) ysm[(c * RV + v) * 32 + lane] = __ldg(p + v);
+        for (int v = 0; v < RV; ++v) reinterpret_cast<V*>(yv)[v] = __ldg(p + v);
+        if (rbf) rbf_center_col<KD>(yv, c0, ralpha);
+#pragma unroll
+        for (int v = 0; v < RV; ++v) ysm[(c * RV + v) * 32 + lane] = reinterpret_cast<V*>(yv)[v];
       }
+      if (rbf) {
+#pragma unroll
+        for (int k = 0; k < KD; ++k) c0[k] = -c0[k];
+      }
+#pragma unroll
+      for (int v = 0; v < RV; ++v) ysm[v * 32 + lane] = reinterpret_cast<V*>(c0)[v];
     };
     auto y_col = [&](int c, T (&yv)[RS]) {
 #pragma unroll
@@ -191,13 +212,29 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
       for (int v = 0; v < RV; ++v) reinterpret_cast<V*>(xv)[v] = __ldg(p + v);
     };
     auto gram_row = [&](const T (&xv)[RS], T (&m)[C], T (&arg)[C]) {
+      if (rbf) {
+        T negc[RS], xt[RS];
+        y_col(0, negc);
+        rbf_center_row<KD>(xv, negc, ralpha, xt);
+        arg[0] = xt[KD];
+        m[0] = kexp2(xt[KD]);
 #pragma unroll
-      for (int c = 0; c < C; ++c) {
-        T yv[RS];
-        y_col(c, yv);
-        const T acc = packed_arg<KD, kPairArg>(xv, yv, T(0));
-        arg[c] = acc;
-        m[c] = rbf ? kexp2(acc) : acc;
+        for (int c = 1; c < C; ++c) {
+          T yv[RS];
+          y_col(c, yv);
+          const T acc = centred_arg<KD, kPairArg>(xt, yv, xt[KD]);
+          arg[c] = acc;
+          m[c] = kexp2(acc);
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+          T yv[RS];
+          y_col(c, yv);
+          const T acc = packed_arg<KD, kPairArg>(xv, yv, T(0));
+          arg[c] = acc;
+          m[c] = acc;
+        }
       }
     };
     auto rec_at = [&](int s, long long t) { return REC + ((long long)s * steps_max + t) * NX * 32; };
@@ -395,9 +432,9 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
 #pragma unroll
       for (int c = 0; c < C; ++c) { Mprev[c] = T(0); argprev[c] = T(0); Zbprev[c] = T(0); }
       T DMlast0 = T(0), mr_old = T(0), ar_old = T(0);
-      T accprev[KD + 1];
+      T accprev[KD];
 #pragma unroll
-      for (int k = 0; k <= KD; ++k) accprev[k] = T(0);
+      for (int k = 0; k < KD; ++k) accprev[k] = T(0);
       T Aprev[NX];
 #pragma unroll
       for (int h = 0; h < NX; ++h) Aprev[h] = T(0);
@@ -428,12 +465,12 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
         T Ain[NX];
 #pragma unroll
         for (int h = 0; h < NX; ++h) Ain[h] = shfl_down(Aprev[h], 1);
-        T acc[KD + 1];
+        T acc[KD];
 #pragma unroll
-        for (int k = 0; k <= KD; ++k) acc[k] = shfl_down(accprev[k], 1);
+        for (int k = 0; k < KD; ++k) acc[k] = shfl_down(accprev[k], 1);
         if (lane == 31) {
 #pragma unroll
-          for (int k = 0; k <= KD; ++k) acc[k] = T(0);
+          for (int k = 0; k < KD; ++k) acc[k] = T(0);
 #pragma unroll
           for (int h = 0; h < NX; ++h)
             Ain[h] = (s + 1 < ns && act) ? brin[(long long)g * NX + h] : T(0);
@@ -683,7 +720,7 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
 
         // ---- grid row p = g + 1: partial Mbar of this lane's cells ----
         const int p = g + 1;
-        T dp = T(0);
+        T dp = T(0), sw = T(0);
 #pragma unroll
         for (int c = 0; c <= C; ++c) {
           T mb, Mq, aq;
@@ -700,28 +737,39 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
           const int q = s * STRIP + C * lane + c;
           const bool valid = fin && q < Ly && (c < C || lane < 31);
           const T W = valid ? (rbf ? mb * Mq : mb) : T(0);
-          T yv[RS];
-          y_col(c, yv);
+          // RBF: column 0 is the lane's centre (y' = 0); sums in the lane's
+          // frame, scaled by 2a (the stored columns are 2a y').
+          if (!rbf || c > 0) {
+            T yv[RS];
+            y_col(c, yv);
 #pragma unroll
-          for (int k = 0; k < KD; ++k) acc[k] = fma(W, yv[k], acc[k]);
-          acc[KD] += W;
+            for (int k = 0; k < KD; ++k) acc[k] = fma(W, yv[k], acc[k]);
+          }
+          sw += W;
           dp = fma(W, rbf ? aq : Mq, dp);
         }
         if (want_dpar) dpar_w += (double)dp;
-        if (lane == 0 && fin) {
-          T xp[RS];
+        if (rbf) {
+          // 2a sum_c W_c (y_c - x_p) = sum_c W_c 2a y'_c - 2a x'_p sum_c W_c:
+          // frame-independent, so the lanes' shares add up along the row.
+          T xp[RS], negc[RS];
           load_x(p, xp);
+          y_col(0, negc);
+          const T t = T(-2) * ralpha * sw;
+#pragma unroll
+          for (int k = 0; k < KD; ++k) acc[k] = fma(xp[k] + negc[k], t, acc[k]);
+        }
+        if (lane == 0 && fin) {
           T* dst = args.dX + ((long long)a * args.LX + p) * args.d;
 #pragma unroll
           for (int k = 0; k < KD; ++k) {
             if (k < args.d) {
-              const T v = rbf ? acc[k] - acc[KD] * (xp[k] * inv2a) : acc[k];
-              atomicAdd(dst + k, xscale_t * v);
+              atomicAdd(dst + k, xscale_t * acc[k]);
             }
           }
         }
 #pragma unroll
-        for (int k = 0; k <= KD; ++k) accprev[k] = acc[k];
+        for (int k = 0; k < KD; ++k) accprev[k] = acc[k];
 #pragma unroll
         for (int h = 0; h < NX; ++h) Aprev[h] = Aout[h];
         DMlast0 = DMnew[0];

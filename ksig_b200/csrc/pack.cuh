@@ -1,15 +1,19 @@
 // Packing of input sequences into the fused-Gram row format.
 //
 // A static-kernel value between point x (row side) and point y (column side)
-// is evaluated by the hot kernels as ONE dot product of packed rows:
-//     arg = xr[KD] + yr[KD] + sum_{k<KD} xr[k] * yr[k]
-//   RBF    (ksig/static/kernels.py:258-260, ksig/utils.py:149-156):
-//          xr = (2a x, -a|x|^2), yr = (y, -a|y|^2), a = log2(e)/max(2s^2,1e-12)
-//          so arg = -a |x-y|^2 and M = exp2(arg) = exp(-|x-y|^2 / max(2s^2,eps)).
-//   linear (ksig/static/kernels.py:155): xr = (s x, 0), yr = (y, 0), M = arg.
+// is evaluated by the hot kernels from packed rows of KD coordinates plus a
+// norm slot at index KD:
+//   RBF    (ksig/static/kernels.py:258-260, ksig/utils.py:149-156): both
+//          sides raw (x, 0) and (y, 0).  The kernels move each lane's points
+//          to a lane-centred frame (rbf_center_cols / rbf_center_row in
+//          common.cuh) and evaluate arg = -a |x - y|^2 with
+//          a = log2(e)/max(2s^2,1e-12), M = exp2(arg).
+//   linear (ksig/static/kernels.py:155): xr = (s x, 0), yr = (y, 0),
+//          arg = xr[KD] + yr[KD] + sum_{k<KD} xr[k] * yr[k], M = arg.
 //   polynomial: as linear with s = 1 (arg = <x, y>); Matern / rational
-//          quadratic: as RBF with a = 1 (arg = -|x-y|^2); the kernel value
-//          is formed by static_value (common.cuh).
+//          quadratic: xr = (2x, -|x|^2), yr = (y, -|y|^2); their sweep
+//          instantiations sum the squared distance from coordinate
+//          differences, and static_value (common.cuh) forms the kernel value.
 // Rows are padded with zeros to KD coordinates and to a 16-byte stride so the
 // kernels read them with vector loads.  Norms are formed in FP64.
 #pragma once
@@ -36,8 +40,7 @@ template <typename T>
 __global__ void pack_rows_kernel(PackArgs a, T* __restrict__ dst) {
   const long long total = (long long)a.n * a.L;
   const bool dist = kind_is_distance(a.kind);
-  const double alpha =
-      a.kind == KIND_RBF ? 1.4426950408889634 / fmax(2.0 * a.param * a.param, 1e-12) : 1.0;
+  const bool raw = a.kind == KIND_RBF;  // centred in the kernels
   const double lin = a.kind == KIND_LINEAR ? a.param : 1.0;
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < total;
        r += (long long)gridDim.x * blockDim.x) {
@@ -58,11 +61,12 @@ __global__ void pack_rows_kernel(PackArgs a, T* __restrict__ dst) {
       }
       nrm += v * v;
       double o;
-      if (dist) o = a.row_side ? 2.0 * alpha * v : v;
+      if (raw) o = v;
+      else if (dist) o = a.row_side ? 2.0 * v : v;
       else o = a.row_side ? lin * v : v;
       out[k] = (T)o;
     }
-    out[a.kd] = (T)(dist ? -alpha * nrm : 0.0);
+    out[a.kd] = (T)(dist && !raw ? -nrm : 0.0);
     for (int k = a.kd + 1; k < a.stride; ++k) out[k] = (T)0;
   }
 }

@@ -112,8 +112,11 @@ pde_bwd_kernel(const PdeBwdArgs<T> args) {
   const double alpha = 1.4426950408889634 / fmax(2.0 * args.param * args.param, 1e-12);
   const bool rbf = args.kind == KIND_RBF;
   const bool want_dpar = args.dparam != nullptr;
-  const T inv2a = T(1.0 / (2.0 * alpha));
-  const double xscale = rbf ? 1.0 / (args.param * args.param) : args.param;
+  const T ralpha = T(alpha);
+  // dM/dx = M (y - x) / s^2 (RBF; the row sums below carry 2a (y - x)) or
+  // s y (linear).
+  const double xscale =
+      rbf ? 1.0 / (args.param * args.param) / (2.0 * alpha) : args.param;
   double dpar_w = 0.0;
 
   for (long long tid = wg; tid < args.ntasks; tid += nw) {
@@ -150,6 +153,8 @@ pde_bwd_kernel(const PdeBwdArgs<T> args) {
 #pragma unroll
         for (int k = 0; k <= KD; ++k) yv[c][k] = tmp[k];
       }
+      // RBF: the lane-centred frame of rbf_center_cols.
+      if (rbf) rbf_center_cols<KD, C + 1>(yv, ralpha);
     };
     auto gram = [&](int row, T (&m)[C + 1], T (&arg)[C + 1]) {
       row = row < 0 ? 0 : (row > lx ? lx : row);
@@ -157,11 +162,22 @@ pde_bwd_kernel(const PdeBwdArgs<T> args) {
       T xv[RS];
 #pragma unroll
       for (int v = 0; v < RS / VN; ++v) reinterpret_cast<V*>(xv)[v] = __ldg(p + v);
+      if (rbf) {
+        T xt[RS];
+        rbf_center_row<KD>(xv, yv[0], ralpha, xt);
+        arg[0] = xt[KD];
+        m[0] = kexp2(xt[KD]);
 #pragma unroll
-      for (int c = 0; c <= C; ++c) {
-        const T acc = packed_arg<KD, false>(xv, yv[c], T(0));
-        arg[c] = acc;
-        m[c] = static_value(acc, args.kind);
+        for (int c = 1; c <= C; ++c) {
+          arg[c] = centred_arg<KD, false>(xt, yv[c], xt[KD]);
+          m[c] = kexp2(arg[c]);
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c <= C; ++c) {
+          arg[c] = packed_arg<KD, false>(xv, yv[c], T(0));
+          m[c] = arg[c];
+        }
       }
     };
 
@@ -268,9 +284,9 @@ pde_bwd_kernel(const PdeBwdArgs<T> args) {
       T Aprev[NB];
 #pragma unroll
       for (int h = 0; h < NB; ++h) Aprev[h] = T(0);
-      T accprev[KD + 1];
+      T accprev[KD];
 #pragma unroll
-      for (int k = 0; k <= KD; ++k) accprev[k] = T(0);
+      for (int k = 0; k < KD; ++k) accprev[k] = T(0);
       T gr_below = T(0), zr_below = T(0);  // lane l+1's G and q one cell row down
       for (int u = 0; u < lx + 33; ++u) {
         const int rho = u - (31 - lane);
@@ -280,12 +296,12 @@ pde_bwd_kernel(const PdeBwdArgs<T> args) {
         T Ain[NB];
 #pragma unroll
         for (int h = 0; h < NB; ++h) Ain[h] = shfl_down(Aprev[h], 1);
-        T acc[KD + 1];
+        T acc[KD];
 #pragma unroll
-        for (int k = 0; k <= KD; ++k) acc[k] = shfl_down(accprev[k], 1);
+        for (int k = 0; k < KD; ++k) acc[k] = shfl_down(accprev[k], 1);
         if (lane == 31) {
 #pragma unroll
-          for (int k = 0; k <= KD; ++k) acc[k] = T(0);
+          for (int k = 0; k < KD; ++k) acc[k] = T(0);
 #pragma unroll
           for (int h = 0; h < NB; ++h)
             Ain[h] = (s + 1 < ns && act) ? __ldcg(brin + (long long)r * NB + h) : T(0);
@@ -440,7 +456,7 @@ pde_bwd_kernel(const PdeBwdArgs<T> args) {
 
         // ---- grid row p = r + 1: partial Mbar of this lane's cells ----
         const int p = r + 1;
-        T dp = T(0);
+        T dp = T(0), sw = T(0);
 #pragma unroll
         for (int c = 0; c <= C; ++c) {
           T mb = (c < C) ? Zbprev[c < C ? c : 0] - Zb[c < C ? c : 0] : T(0);
@@ -448,28 +464,36 @@ pde_bwd_kernel(const PdeBwdArgs<T> args) {
           const int q = g0 + c;
           const bool valid = fin && q < Ly && (c < C || lane < 31);
           const T W = valid ? (rbf ? mb * Mprev[c] : mb) : T(0);
+          // RBF: column 0 is the lane's centre (y' = 0); the other columns
+          // hold 2a y' in the lane's frame.
+          if (!rbf || c > 0) {
 #pragma unroll
-          for (int k = 0; k < KD; ++k) acc[k] = fma(W, yv[c][k], acc[k]);
-          acc[KD] += W;
+            for (int k = 0; k < KD; ++k) acc[k] = fma(W, yv[c][k], acc[k]);
+          }
+          sw += W;
           dp = fma(W, rbf ? argprev[c] : Mprev[c], dp);
         }
         if (want_dpar) dpar_w += (double)dp;
-        if (lane == 0 && fin) {
-          const V* xp = reinterpret_cast<const V*>(xb + (long long)p * RS);
+        if (rbf) {
+          // 2a sum_c W_c (y_c - x_p) = sum_c W_c 2a y'_c - 2a x'_p sum_c W_c:
+          // frame-independent, so the lanes' shares add up along the row.
+          const V* xp = reinterpret_cast<const V*>(xb + (long long)(p < 0 ? 0 : (p < lx ? p : lx)) * RS);
           T xv[RS];
 #pragma unroll
           for (int v = 0; v < RS / VN; ++v) reinterpret_cast<V*>(xv)[v] = __ldg(xp + v);
+          const T t = T(-2) * ralpha * sw;
+#pragma unroll
+          for (int k = 0; k < KD; ++k) acc[k] = fma(xv[k] + yv[0][k], t, acc[k]);
+        }
+        if (lane == 0 && fin) {
           T* dst = args.dX + ((long long)a * args.LX + p) * args.d;
 #pragma unroll
           for (int k = 0; k < KD; ++k) {
-            if (k < args.d) {
-              const T v = rbf ? acc[k] - acc[KD] * (xv[k] * inv2a) : acc[k];
-              atomicAdd(dst + k, (T)(xscale * (double)v));
-            }
+            if (k < args.d) atomicAdd(dst + k, (T)(xscale * (double)acc[k]));
           }
         }
 #pragma unroll
-        for (int k = 0; k <= KD; ++k) accprev[k] = acc[k];
+        for (int k = 0; k < KD; ++k) accprev[k] = acc[k];
         gr_below = Ain[F];
         zr_below = Ain[2 * F];
 #pragma unroll

@@ -35,7 +35,24 @@ struct PlainArgs {
   T* scratch;            // per CTA: (2 + 2 p^2) arrays of cap floats
   long long cap;         // floats per array (>= max lx * ly)
   int* status;
+  T ralpha;              // RBF: log2(e) / max(2 s^2, 1e-12)
 };
+
+// Static-kernel argument of two packed points (pack.cuh): RBF rows are raw,
+// arg = -a |x - y|^2; linear arg = <s x, y>.
+template <typename T>
+__device__ __forceinline__ T plain_arg(const T* x, const T* y, int kd, int kind, T ralpha) {
+  T acc = T(0);
+  if (kind == KIND_RBF) {
+    for (int k = 0; k < kd; ++k) {
+      const T v = x[k] - y[k];
+      acc = fma(v, v, acc);
+    }
+    return -ralpha * acc;
+  }
+  for (int k = 0; k < kd; ++k) acc = fma(x[k], y[k], acc);
+  return acc;
+}
 
 template <typename T>
 __device__ T block_sum(T v, T* sh) {
@@ -116,9 +133,7 @@ __global__ void __launch_bounds__(256) plain_dp_kernel(const PlainArgs<T> a) {
     auto Mv = [&](int i, int j) {
       const T* x = xb + (long long)i * a.rs;
       const T* y = yb + (long long)j * a.rs;
-      T acc = x[a.kd] + y[a.kd];
-      for (int k = 0; k < a.kd; ++k) acc = fma(x[k], y[k], acc);
-      return static_value(acc, a.kind);
+      return static_value(plain_arg(x, y, a.kd, a.kind, a.ralpha), a.kind);
     };
     for (long long e = threadIdx.x; e < (long long)lx * ly; e += blockDim.x) {
       const int i = (int)(e / ly), j = (int)(e - (long long)i * ly);
@@ -305,9 +320,7 @@ __global__ void __launch_bounds__(256) plain_dp_bwd_kernel(const PlainBwdArgs<T>
     auto argv = [&](int i, int j) {
       const T* x = xb + (long long)i * a.rs;
       const T* y = yb + (long long)j * a.rs;
-      T acc = x[a.kd] + y[a.kd];
-      for (int k = 0; k < a.kd; ++k) acc = fma(x[k], y[k], acc);
-      return acc;
+      return plain_arg(x, y, a.kd, a.kind, a.ralpha);
     };
     auto Mv = [&](int i, int j) { return static_value(argv(i, j), a.kind); };
     auto wk = [&](int k) {
@@ -489,7 +502,6 @@ __global__ void __launch_bounds__(256) plain_dp_bwd_kernel(const PlainBwdArgs<T>
     }
     __syncthreads();
     const double sc = rbf ? 1.0 / (ba.param * ba.param) : ba.param;
-    const T inv2a = T(1.0 / (2.0 * alpha));
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nwp = blockDim.x >> 5;
     for (int i = wp; i < Gx; i += nwp) {
       const T* xr = xb + (long long)i * a.rs;
@@ -505,7 +517,7 @@ __global__ void __launch_bounds__(256) plain_dp_bwd_kernel(const PlainBwdArgs<T>
           sw += __shfl_xor_sync(FULL, sw, o);
         }
         if (lane == 0) {
-          const T v = rbf ? acc - sw * (xr[k] * inv2a) : acc;
+          const T v = rbf ? acc - sw * xr[k] : acc;
           atomicAdd(ba.dX + ((long long)ab.x * ba.LX + i) * ba.d + k, (T)(sc * (double)v));
         }
       }

@@ -56,6 +56,15 @@ struct SweepArgs {
   int nX, nYseq;         // sequence counts (bounds of LIST pairs)
   int* status;
   StaticParams sp;       // epilogue constants of the other static kernels (EXT)
+  T ralpha;              // RBF: log2(e) / max(2 s^2, 1e-12) (lane-centred Gram)
+  // Gram-input instantiations (KD == 0): static-kernel values precomputed
+  // by gram_kernel (gram.cuh), one [rows][gram_ld] slot per task of this
+  // launch; the launch covers task positions task_base .. task_base +
+  // ntasks - 1 of a call with ntasks_total tasks.
+  const T* gram;
+  long long gram_slot;   // elements per slot
+  int gram_ld;           // row stride of a slot
+  int task_base, ntasks_total;
 };
 
 // Item geometry a policy may need.
@@ -68,7 +77,7 @@ struct ItemInfo {
 // (sweep_dyn_smem_bytes on the host).
 template <typename T, int KD, int C>
 struct SweepSmem {
-  static constexpr int RS = packed_stride<T>(KD);
+  static constexpr int RS = KD == 0 ? 1 : packed_stride<T>(KD);
   T ynext[32][C * RS];
 };
 
@@ -76,7 +85,10 @@ template <typename T, int KD, int C, bool DIFF, int WPB, bool EXT, class Policy>
 __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
                                       SweepSmem<T, KD, C>& sm) {
   constexpr int NX = Policy::NX;
-  constexpr int RS = packed_stride<T>(KD);
+  // KD == 0: Gram input.  The per-step "x row" of a lane is then its C
+  // static-kernel values of that grid row, read from the task's Gram slot.
+  constexpr bool GIN = KD == 0;
+  constexpr int RS = GIN ? C : packed_stride<T>(KD);
   constexpr int VN = Vec<T>::N;
   using V = typename Vec<T>::type;
   constexpr int STRIP = DIFF ? 32 * C - 1 : 32 * C;
@@ -100,17 +112,18 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
     const long long tid = wg + q * nw;
     if (tid >= args.ntasks) {
       it.task = -1; it.b = 0; it.Lx = 1; it.Ly = 1; it.rows = 16; it.ns = 1;
-      it.xb = args.xr;
+      it.xb = GIN ? args.gram : args.xr;
       return;
     }
-    it.task = args.order ? args.order[tid] : (int)tid;
-    int2 ab = decode_task((int)tid, args.mode, args.nY, args.list, args.order);
+    const int pos = args.task_base + (int)tid;
+    it.task = args.order ? args.order[pos] : pos;
+    int2 ab = decode_task(pos, args.mode, args.nY, args.list, args.order);
     if (ab.x < 0 || ab.x >= args.nX || ab.y < 0 || ab.y >= args.nYseq) {
       set_status(args.status, KSIG_ERR_INVALID);  // pair index out of range
       ab = make_int2(0, 0);
     }
     it.b = ab.y;
-    it.xb = args.xr + args.xstart[ab.x] * RS;
+    it.xb = GIN ? args.gram + tid * args.gram_slot : args.xr + args.xstart[ab.x] * RS;
     it.Lx = args.xlen[ab.x];
     it.Ly = args.ylen[ab.y];
     const int lx = DIFF ? it.Lx - 1 : it.Lx;
@@ -134,7 +147,7 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
   };
   // Stages the lane's column points of `it` into its smem slot.
   auto stage_y = [&](const Item& it) {
-    if (it.task < 0) return;
+    if (GIN || it.task < 0) return;
 #pragma unroll
     for (int c = 0; c < C; ++c) {
       const T* src = ycol_ptr(it, c);
@@ -146,7 +159,10 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
   };
 
   T yv[C][KD + 1];
+  // RBF: the lane's columns in its centred frame (rbf_center_cols).
+  const bool centred = !EXT && args.kind == KIND_RBF;
   auto y_from_slot = [&]() {
+    if constexpr (GIN) return;
     __pipeline_wait_prior(0);
 #pragma unroll
     for (int c = 0; c < C; ++c) {
@@ -157,20 +173,42 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
 #pragma unroll
       for (int k = 0; k <= KD; ++k) yv[c][k] = tmp[k];
     }
+    if (centred) rbf_center_cols<KD, C>(yv, args.ralpha);
   };
-  auto load_x = [&](const T* xb, int Lx, int row, T (&xv)[RS]) {
-    row = row < Lx - 1 ? row : Lx - 1;
-    const V* p = reinterpret_cast<const V*>(xb + (long long)row * RS);
+  auto load_x = [&](const Item& it, int row, T (&xv)[RS]) {
+    row = row < it.Lx - 1 ? row : it.Lx - 1;
+    if constexpr (GIN) {
+      // The lane's C Gram values of grid row `row` (columns past the
+      // sequence's end repeat its last column, as the points do).
+      const T* p = it.xb + (long long)row * args.gram_ld;
+      const int c0 = it.s * STRIP + C * lane;
 #pragma unroll
-    for (int v = 0; v < RS / VN; ++v) reinterpret_cast<V*>(xv)[v] = __ldg(p + v);
+      for (int c = 0; c < C; ++c) xv[c] = __ldg(p + (c0 + c < it.Ly - 1 ? c0 + c : it.Ly - 1));
+    } else {
+      const V* p = reinterpret_cast<const V*>(it.xb + (long long)row * RS);
+#pragma unroll
+      for (int v = 0; v < RS / VN; ++v) reinterpret_cast<V*>(xv)[v] = __ldg(p + v);
+    }
   };
   // Static-kernel values of one grid row; call sites pass a literal for RBF,
-  // so after inlining the steady loop carries no per-point select.
+  // so after inlining the steady loop carries no per-point select.  RBF
+  // rows are moved to the lane's centred frame first; column 0 is the
+  // centre itself (arg = -a |x'|^2, no dot product).
   auto gram = [&](bool RBF, const T (&xv)[RS], T (&m)[C]) {
+    if constexpr (GIN) {
 #pragma unroll
-    for (int c = 0; c < C; ++c) {
-      const T acc = packed_arg<KD, kPairArg>(xv, yv[c], T(0));
-      m[c] = RBF ? kexp2(acc) : acc;
+      for (int c = 0; c < C; ++c) m[c] = xv[c];
+    } else {
+      if (RBF) {
+        T xt[RS];
+        rbf_center_row<KD>(xv, yv[0], args.ralpha, xt);
+        m[0] = kexp2(xt[KD]);
+#pragma unroll
+        for (int c = 1; c < C; ++c) m[c] = kexp2(centred_arg<KD, kPairArg>(xt, yv[c], xt[KD]));
+      } else {
+#pragma unroll
+        for (int c = 0; c < C; ++c) m[c] = packed_arg<KD, kPairArg>(xv, yv[c], T(0));
+      }
     }
   };
   // Runtime-kind version for the rare paths (one copy of the code).  The
@@ -195,18 +233,16 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
           }
         }
         m[c] = static_value_other(acc, args.kind, args.sp);
-      } else {
-        const T acc = packed_arg<KD, kPairArg>(xv, yv[c], T(0));
-        m[c] = static_value(acc, args.kind);
       }
     }
+    if constexpr (!EXT) gram(centred, xv, m);
   };
 
   Item cur, nxt;
   make_item(0, cur);
   next_of(cur, nxt);
   // First item's columns straight into registers; the next item is staged.
-  if (cur.task >= 0) {
+  if (!GIN && cur.task >= 0) {
 #pragma unroll
     for (int c = 0; c < C; ++c) {
       const V* p = reinterpret_cast<const V*>(ycol_ptr(cur, c));
@@ -216,6 +252,7 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
 #pragma unroll
       for (int k = 0; k <= KD; ++k) yv[c][k] = tmp[k];
     }
+    if (centred) rbf_center_cols<KD, C>(yv, args.ralpha);
   } else {
 #pragma unroll
     for (int c = 0; c < C; ++c)
@@ -225,14 +262,15 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
   stage_y(nxt);
 
   const bool rbf = args.kind == KIND_RBF;
-  const bool fast = !EXT && (rbf || args.kind == KIND_LINEAR);
+  // Gram input serves every static kind through the steady loop.
+  const bool fast = GIN || (!EXT && (rbf || args.kind == KIND_LINEAR));
   T Mcur[C], DMcur[C], Mtmp[C], DMtmp[C];
   T xv[RS];
-  load_x(cur.xb, cur.Lx, 0, xv);
+  load_x(cur, 0, xv);
   gram_rt(xv, Mcur);
 #pragma unroll
   for (int c = 0; c < C; ++c) DMcur[c] = T(0);
-  load_x(cur.xb, cur.Lx, 1, xv);  // Gram row of the first step
+  load_x(cur, 1, xv);  // Gram row of the first step
 
   // Cell work recorded at one step and executed at the next, so that a
   // step's Gram and its cell recursion form one branch-free block the
@@ -300,9 +338,9 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
   // two-deep x prefetch of the unrolled steady loop.
   auto load_x2 = [&](T (&dst)[RS]) {
     const int u1 = u + 1;
-    if (u1 < cur.rows) load_x(cur.xb, cur.Lx, u1 + 1, dst);
-    else if (u1 == cur.rows) load_x(nxt.xb, nxt.Lx, 0, dst);
-    else load_x(nxt.xb, nxt.Lx, 1, dst);
+    if (u1 < cur.rows) load_x(cur, u1 + 1, dst);
+    else if (u1 == cur.rows) load_x(nxt, 0, dst);
+    else load_x(nxt, 1, dst);
   };
   // One step of the steady loop (see below).
   auto steady_step = [&](int rbf_c, T (&Mc)[C], T (&Mn)[C], T (&DMc)[C], T (&DMn)[C]) {
@@ -312,7 +350,7 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
     pr = u - 1;
     ++u;
     const bool sw = (u == cur.rows);
-    load_x(sw ? nxt.xb : cur.xb, sw ? nxt.Lx : cur.Lx, sw ? 0 : u + 1, xv);
+    load_x(sw ? nxt : cur, sw ? 0 : u + 1, xv);
   };
   // Same, with this step's x row in xa, refilled afterwards with the row two
   // steps ahead (hides the strided row loads behind a whole step).
@@ -337,7 +375,7 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
         for (int k = 0; k < RS; ++k) xa[k] = xv[k];
         {
           const bool sw = (u + 1 == cur.rows);
-          load_x(sw ? nxt.xb : cur.xb, sw ? nxt.Lx : cur.Lx, sw ? 0 : u + 2, xb2);
+          load_x(sw ? nxt : cur, sw ? 0 : u + 2, xb2);
         }
         for (; it + 1 < n; it += 2) {  // unrolled by two: buffers swap roles
           steady_step2(rbf_c, Mcur, Mtmp, DMcur, DMtmp, xa);
@@ -445,7 +483,7 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
     // Prefetch the x row of the next step's Gram.
     {
       const bool sw = (u == cur.rows);
-      load_x(sw ? nxt.xb : cur.xb, sw ? nxt.Lx : cur.Lx, sw ? 0 : u + 1, xv);
+      load_x(sw ? nxt : cur, sw ? 0 : u + 1, xv);
     }
     if (delay > 0) --delay;
   }
@@ -690,7 +728,7 @@ dp_fwd_kernel(const SweepArgs<T> args) {
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   auto* sm = reinterpret_cast<SweepSmem<T, KD, C>*>(dyn_smem);
   DpPolicy<T, C, NL, P, WPB> pol;
-  pol.init(red[threadIdx.x >> 5], args.out, args.ntasks, args.nl_out);
+  pol.init(red[threadIdx.x >> 5], args.out, args.ntasks_total, args.nl_out);
   sweep<T, KD, C, DIFF, WPB, EXT>(args, pol, sm[threadIdx.x >> 5]);
 }
 

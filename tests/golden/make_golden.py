@@ -1,9 +1,9 @@
 """Generates the golden fixtures in this folder from the reference KSig itself.
 
 Run from the repository root, in a container that has the reference source
-checked out at ``--ref`` (default ``/root/reference``)::
+checked out at ``--ref`` (a path to the KSig 1.0.0 source tree)::
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <path to the KSig source tree>
 
 The reference needs CuPy and a CUDA device.  Neither is needed here: the
 NumPy-backed ``cupy`` stand-in in ``tests/_refshim`` takes CuPy's place and
@@ -117,12 +117,46 @@ def _cases():
   add('pde_poly', 'pde', dict(normalize=False, static='poly', param=[2.0, 1.0, 0.3]),
       P[:, :6], Q[:, :5])
 
+  # Full order beyond 4 (order 0 -> order = n_levels, ksig/kernels.py:
+  # 49-50), deeper truncations, and more channels than the register-Gram
+  # tiles hold (the Gram-input path).
+  add('dp_ofull_m6_norm', 'sig', dict(n_levels=6, order=0, normalize=True,
+                                       static='rbf', param=0.9), X1, Y1)
+  add('dp_o5_m8', 'sig', dict(n_levels=8, order=5, normalize=False,
+                               static='rbf', param=1.1), X1[:, :11], Y1[:, :9])
+  add('dp_ofull_m10', 'sig', dict(n_levels=10, order=0, normalize=False,
+                                   static='rbf', param=1.0), X1[:3, :8], Y1[:2, :7])
+  add('dp_m16_norm', 'sig', dict(n_levels=16, order=1, normalize=True,
+                                  static='rbf', param=0.8), X1, Y1)
+  add('dp_o2_m12', 'sig', dict(n_levels=12, order=2, normalize=False,
+                                static='rbf', param=0.8), X1, Y1)
+  rng = np.random.default_rng(15)
+  W1 = np.cumsum(rng.standard_normal((4, 23, 64)) * 0.2, axis=1)
+  W2 = np.cumsum(rng.standard_normal((3, 19, 64)) * 0.2, axis=1)
+  add('dp_d64_norm', 'sig', dict(n_levels=4, order=1, normalize=True,
+                                  static='rbf', param=2.0), W1, W2)
+  add('dp_d64_o2', 'sig', dict(n_levels=4, order=2, normalize=False,
+                                static='rbf', param=2.0), W1, W2)
+  add('dp_d40_linear', 'sig', dict(n_levels=3, order=1, normalize=True,
+                                    static='linear', param=0.3),
+      W1[:, :, :40], W2[:, :, :40])
+  add('dp_d40_matern52', 'sig', dict(n_levels=4, order=1, normalize=False,
+                                      static='matern52', param=2.5),
+      W1[:, :, :40], W2[:, :, :40])
+  add('dp_d64_ragged', 'sig', dict(n_levels=4, order=1, normalize=True,
+                                    static='rbf', param=2.0),
+      [W1[0, :9], W1[1], W1[2, :15]], [W2[0, :4], W2[1], W2[2, :12]], ragged=True)
+  add('pde_d48_norm', 'pde', dict(normalize=True, static='rbf', param=2.0),
+      W1[:, :, :48], W2[:, :, :48])
+
   # Global alignment kernel (ksig/kernels.py:366-409).
   rng = np.random.default_rng(14)
   G1 = np.cumsum(rng.standard_normal((4, 11, 3)) * 0.4, axis=1)
   G2 = np.cumsum(rng.standard_normal((3, 8, 3)) * 0.4, axis=1)
   add('ga_rbf', 'ga', dict(normalize=True, static='rbf', param=1.2), G1, G2)
   add('ga_linear', 'ga', dict(normalize=True, static='linear', param=0.4), G1, G2)
+  add('ga_d40', 'ga', dict(normalize=True, static='rbf', param=3.0),
+      W1[:, :11, :40], W2[:, :8, :40])
   return cases
 
 
@@ -227,7 +261,8 @@ def _run_preprocessing():
 
 def main():
   ap = argparse.ArgumentParser()
-  ap.add_argument('--ref', default='/root/reference')
+  ap.add_argument('--ref', required=True,
+                  help='KSig 1.0.0 source tree (the directory holding ksig/)')
   ap.add_argument('--_child', action='store_true')
   a = ap.parse_args()
   if a._child:
@@ -238,7 +273,7 @@ def main():
   env['PYTHONPATH'] = os.pathsep.join([SHIM, a.ref])
   env['NUMBA_ENABLE_CUDASIM'] = '1'
   subprocess.run([sys.executable, '-W', 'ignore', os.path.abspath(__file__),
-                  '--_child'], env=env, check=True, cwd='/tmp')
+                  '--ref', a.ref, '--_child'], env=env, check=True, cwd='/tmp')
 
 
 if __name__ == '__main__':

@@ -54,6 +54,49 @@ def test_static_scratch_entry_matches_workspace_entry():
     assert _rel(out, ref) < TOL, f'call {call}'
 
 
+@pytest.mark.parametrize('dtype', ['f32', 'f64'])
+def test_static_scratch_entry_ragged(dtype):
+  """Ragged lengths (natural task order, lengths resolved in the shared
+  array) and the FP64 path, two calls in a row, against
+  ksig_signature_kern; then a length outside [1, L] is clamped, flagged in
+  the array's status word and reported by ksig_static_status."""
+  from ksig_b200 import _engine as E
+  from ksig_b200 import _lib as L
+  lib = L.lib()
+  tdt = torch.float32 if dtype == 'f32' else torch.float64
+  code = L.DTYPE_F32 if dtype == 'f32' else L.DTYPE_F64
+  tol = TOL if dtype == 'f32' else 1e-10
+  stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+  for call, (seed, nx, ny, Lx, Ly) in enumerate([(3, 5, 4, 70, 50), (4, 3, 6, 40, 300)]):
+    X = torch.as_tensor(_walks(seed, nx, Lx, 2), device='cuda').to(tdt)
+    Y = torch.as_tensor(_walks(seed + 5, ny, Ly, 2), device='cuda').to(tdt)
+    rng = np.random.default_rng(seed)
+    lx = torch.tensor(rng.integers(1, Lx + 1, nx), dtype=torch.int32, device='cuda')
+    ly = torch.tensor(rng.integers(1, Ly + 1, ny), dtype=torch.int32, device='cuda')
+    Xs, Ys = E.Seqs(X, lx), E.Seqs(Y, ly)
+    ref = E.sig_levels(Xs, Ys, L.PAIRS_FULL, 3, 2, True, L.STATIC_RBF, 0.7)
+    out = torch.full_like(ref, float('nan'))
+    rc = lib.ksig_signature_kern_static(
+        ctypes.c_void_p(X.data_ptr()), ctypes.c_void_p(lx.data_ptr()), nx, Lx,
+        ctypes.c_void_p(Y.data_ptr()), ctypes.c_void_p(ly.data_ptr()), ny, Ly, 2, code,
+        L.STATIC_RBF, 0.7, 3, 2, 1, L.PAIRS_FULL, None, 0,
+        ctypes.c_void_p(out.data_ptr()), stream)
+    assert rc == L.OK, L.last_error()
+    assert lib.ksig_static_status(stream) == L.OK
+    assert torch.isfinite(out).all(), f'call {call}: unwritten output'
+    assert _rel(out, ref) < tol, f'call {call}'
+  # A length past L: clamped on the device and reported.
+  bad = torch.tensor([Lx + 5] + [2] * (nx - 1), dtype=torch.int32, device='cuda')
+  rc = lib.ksig_signature_kern_static(
+      ctypes.c_void_p(X.data_ptr()), ctypes.c_void_p(bad.data_ptr()), nx, Lx,
+      ctypes.c_void_p(Y.data_ptr()), None, ny, Ly, 2, code,
+      L.STATIC_RBF, 0.7, 3, 2, 1, L.PAIRS_FULL, None, 0,
+      ctypes.c_void_p(out.data_ptr()), stream)
+  assert rc == L.OK
+  assert lib.ksig_static_status(stream) == L.ERR_INVALID
+  assert lib.ksig_static_status(stream) == L.OK  # read and cleared
+
+
 def test_static_scratch_entry_rejects_oversized_calls():
   from ksig_b200 import _lib as L
   lib = L.lib()
