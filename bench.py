@@ -181,6 +181,41 @@ def _other_bounds(traffic, k_ms):
   return out
 
 
+def bwd_roofline(bwd_ms, peak):
+  """Roofline of the one-launch DP adjoint on the 512 x 512 levels.
+
+  Algorithmic flops per pair, with G = L^2 grid points and cells = (L-1)^2:
+    phase 1 (forward recomputed):  G (2d + 4) + cells (4 + 4 (m - 1))
+    phase 2 Gram recomputed:       G (2d + 4)
+    state recovery by subtraction: cells 2 (m - 1)
+    adjoint recursion:             cells (5 (m - 1) + 2)
+    pull-back to dX:               G (2d + 6)
+  The per-step records (phase 1 writes, phase 2 reads (L + 33) (m - 1)
+  FP32 values per lane and strip) are the adjoint's own intermediate, not
+  input bytes."""
+  d = D_WALK + 1
+  m = N_LEVELS
+  G = SEQ_LEN * SEQ_LEN
+  cells = (SEQ_LEN - 1) ** 2
+  flops = (2 * G * (2 * d + 4) + G * (2 * d + 6)
+           + cells * ((4 + 4 * (m - 1)) + 2 * (m - 1) + 5 * (m - 1) + 2))
+  achieved = flops * N_SEQ * N_SEQ / (bwd_ms * 1e-3) / 1e12
+  rec = (SEQ_LEN + 33) * (m - 1) * 32 * 4
+  traffic = None
+  tpath = os.path.join(ROOT, 'profiles', 'dp_bwd_traffic.json')
+  if os.path.exists(tpath):
+    with open(tpath) as f:
+      traffic = json.load(f).get('bytes_per_launch')
+  return {'bound': 'fp32', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
+          'frac': achieved / peak if peak else None,
+          'kernel': 'dp_bwd_kernel (one launch, both phases, 512x512 pairs)',
+          'kernel_ms': bwd_ms, 'flops_per_pair': flops,
+          'record_bytes_per_pair': 2 * rec,
+          'traffic': traffic,
+          'traffic_source': ('ncu capture committed as profiles/dp_bwd_traffic.json '
+                             '(not measured in this run)') if traffic else None}
+
+
 def run_ours(args, rank, world, dist):
   import torch
 
@@ -421,6 +456,7 @@ def run_ours(args, rank, world, dist):
             'what': 'plain FP32 one-pair-per-block kernels '
                     '(ksig_signature_kern_plain, ksig_signature_kern_plain_bwd) '
                     'against the fused sweep and adjoint on the same 512x512 levels'},
+        'roofline_bwd': None if bwd_ms is None else bwd_roofline(bwd_ms, peak.value),
         'fwd_bwd': None if fb_ms is None else {
             's_per_step': fb_ms * 1e-3, 'ms_per_step': fb_ms,
             'what': 'K(X, Y) forward + dL/dX backward (L = sum W*K), '
@@ -586,6 +622,74 @@ def run_ragged(args):
   line = {'metric': METRIC}
   line.update(ragged_record(args, args.steps, args.bwd_steps))
   print(json.dumps(line))
+
+
+# Gram forms (not the default bench line): the same DP level computation
+# (N = M = 256 random walks + time, L = 200, RBF bandwidth sqrt(d),
+# n_levels = 5, order 1) at d = 8, 15, 31 and 63 channels plus time, with
+# the static Gram formed three ways:
+#   register: fused in the sweep on the FP32 pipe (FFMA2, lane-centred);
+#   tensor:   tcgen05 3xTF32 tiles into per-task Gram slots, then the
+#             Gram-input sweep (KSIG_FORCE_GIN=1, KSIG_GRAM_TC=1);
+#   cuda:     CUDA-core difference tiles into the slots, then the same sweep.
+# Reports kernel time per form and the largest level difference against the
+# FP64 register path (the forms' oracle errors are in the tests).
+
+def run_gram_forms(args):
+  import torch
+
+  from ksig_b200 import _engine as E
+  from ksig_b200 import _lib as Lb
+  n = args.n_seq or 256
+  dev = torch.device('cuda', 0)
+  out = {'metric': METRIC, 'workload': f'gram_forms_N{n}_L200_m5_p1', 'forms': {}}
+
+  def timed(fn, reps=3):
+    fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+      a = torch.cuda.Event(enable_timing=True)
+      b = torch.cuda.Event(enable_timing=True)
+      a.record()
+      fn()
+      b.record()
+      b.synchronize()
+      ts.append(a.elapsed_time(b))
+    return min(ts)
+
+  for dw in (8, 15, 31, 63):
+    d = dw + 1
+    bw = math.sqrt(dw)
+    X = torch.as_tensor(make_walks(n, SEQ_LEN, dw, 11), device=dev)
+    Y = torch.as_tensor(make_walks(n, SEQ_LEN, dw, 12), device=dev)
+    Xs, Ys = E.Seqs(X), E.Seqs(Y)
+    ref = E.sig_levels(E.Seqs(X.double()), E.Seqs(Y.double()), Lb.PAIRS_FULL, 5, 1, True,
+                       Lb.STATIC_RBF, bw)
+    scale = ref.abs().amax(dim=1, keepdim=True).clamp_min(1e-300)
+    row = {}
+    for form, env in (('register', {}), ('tensor', {'KSIG_FORCE_GIN': '1', 'KSIG_GRAM_TC': '1'}),
+                      ('cuda', {'KSIG_FORCE_GIN': '1', 'KSIG_GRAM_TC': '0'})):
+      if form == 'register' and d > 32:
+        row[form] = {'unavailable': 'no register-Gram tile above 32 coordinates'}
+        continue
+      old = {k: os.environ.get(k) for k in ('KSIG_FORCE_GIN', 'KSIG_GRAM_TC')}
+      os.environ.update(env)
+      try:
+        fn = lambda: E.sig_levels(Xs, Ys, Lb.PAIRS_FULL, 5, 1, True, Lb.STATIC_RBF, bw)  # noqa: E731
+        lev = fn()
+        ms = timed(fn)
+        row[form] = {'ms': ms, 'max_level_diff_vs_fp64': float(((lev - ref).abs() / scale).max())}
+      except Exception as e:  # noqa: BLE001 - a form without a compiled tile
+        row[form] = {'unavailable': str(e)[:120]}
+      finally:
+        for k, v in old.items():
+          if v is None:
+            os.environ.pop(k, None)
+          else:
+            os.environ[k] = v
+    out['forms'][f'd={d}'] = row
+  print(json.dumps(out))
 
 
 # Ragged PDE workload (not the default bench line): N = M = 256 Brownian
@@ -827,7 +931,7 @@ def main():
                   help='skip the ragged order-2 sub-record of the bench line')
   ap.add_argument('--bwd-steps', type=int, default=5)
   ap.add_argument('--workload', default='dp512',
-                  choices=['dp512', 'ragged-dp', 'ragged-pde', 'mmd-pde'],
+                  choices=['dp512', 'ragged-dp', 'ragged-pde', 'mmd-pde', 'gram-forms'],
                   help='dp512: the bench line; ragged-dp: the 2048 x 2048 ragged '
                        'order-2 workload, printed as its own report line')
   ap.add_argument('--plain-sample', type=int, default=96)
@@ -862,6 +966,9 @@ def main():
     return
   if args.workload == 'mmd-pde':
     run_mmd_pde(args)
+    return
+  if args.workload == 'gram-forms':
+    run_gram_forms(args)
     return
   try:
     run_ours(args, rank, world, dist)

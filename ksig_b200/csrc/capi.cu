@@ -19,6 +19,7 @@
 #include "pde_bwd.cuh"
 #include "plain.cuh"
 #include "gram.cuh"
+#include "gram_tc.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
 
@@ -371,7 +372,11 @@ int plan_fwd(int family, int nX, int LX, int nY, int LY, int d, int dtype, int n
   const int op = ga ? OP_GA_FWD
                    : ext ? (pde ? OP_PDE_FWD_EXT : OP_DP_FWD_EXT) : (pde ? OP_PDE_FWD : OP_DP_FWD);
   const int want = want_cols(ly_cells, 8, op);
-  const KernelEntry* k = layout_only ? nullptr : find_kernel(op, pl.f64, d, want, need_nl, p, pl.diff);
+  // KSIG_FORCE_GIN=1 takes the Gram-input path even where a register-Gram
+  // tile exists (measurement of the two Gram forms on the same shapes).
+  const KernelEntry* k = (layout_only || env_int("KSIG_FORCE_GIN", 0))
+                             ? nullptr
+                             : find_kernel(op, pl.f64, d, want, need_nl, p, pl.diff);
   if (layout_only) {
     pl.k = nullptr;
     pl.kd = round_up(d, 4);
@@ -388,7 +393,7 @@ int plan_fwd(int family, int nX, int LX, int nY, int LY, int d, int dtype, int n
     layout_fwd(pl, nX, LX, nY, LY);
     return KSIG_OK;
   }
-  if (!k) {
+  if (!k && !layout_only) {
     // No register-Gram tile for this shape (e.g. more channels than the
     // widest compiled one): the Gram-input instantiation of the same family
     // with a precomputed Gram (any static kind, any d).
@@ -513,6 +518,10 @@ int run_fwd(const FwdPlan& pl, const void* X, const int32_t* lenX, int nX, int L
   a.ntasks = (int)pl.ntasks;
   a.ntasks_total = (int)pl.ntasks;
   a.task_base = 0;
+  // Row prefetch distance (steps ahead): the Gram-input sweeps read a new
+  // slot row every step in every lane (4 steps: 4 % faster on B200); the
+  // register-Gram sweeps gained nothing from it.
+  a.x_prefetch = env_int("KSIG_XPF", pl.gin ? 4 : 0);
   a.kind = kind;
   a.sp = sp;
   a.ralpha = (T)rbf_alpha(kind, param);
@@ -538,16 +547,42 @@ int run_fwd(const FwdPlan& pl, const void* X, const int32_t* lenX, int nX, int L
   g.kind = kind; g.ralpha = a.ralpha; g.sp = sp;
   g.gram = reinterpret_cast<T*>(ws + pl.off_gram);
   g.slot = pl.gram_slot; g.ld = pl.gram_ld;
-  const int tiles_x = (pl.gram_rows + kGramTile - 1) / kGramTile;
-  g.tiles_y = (pl.gram_ld + kGramTile - 1) / kGramTile;
+  // The CUDA-core difference tiles (gram.cuh) by default; RBF in FP32 with
+  // KSIG_GRAM_TC=1: the tensor-core tiles (gram_tc.cuh).  The tensor-core
+  // form centres once per 32 columns and carries 3xTF32 products, so it is
+  // less accurate than the difference tiles on widely spread paths, and the
+  // sweep's reads of the slots, not the Gram, bound this path's time.
+  bool tc = false;
+  if constexpr (std::is_same<T, float>::value)
+    tc = kind == KIND_RBF && env_int("KSIG_GRAM_TC", 0) != 0;
+  const int tm = tc ? kTcM : kGramTile, tn = tc ? kTcN : kGramTile;
+  const int tiles_x = (pl.gram_rows + tm - 1) / tm;
+  g.tiles_y = (pl.gram_ld + tn - 1) / tn;
   g.status = status;
+  if constexpr (std::is_same<T, float>::value) {
+    if (tc) {
+      cudaError_t ce = ensure_smem_attr((const void*)&gram_tc_kernel, gram_tc_smem_bytes());
+      if (ce != cudaSuccess) return cuda_fail(ce, "cudaFuncSetAttribute(gram_tc_kernel)");
+    }
+  }
   a.gram = g.gram; a.gram_slot = pl.gram_slot; a.gram_ld = pl.gram_ld;
   for (long long t0 = 0; t0 < pl.ntasks; t0 += pl.gram_chunk) {
     const long long nt = pl.ntasks - t0 < pl.gram_chunk ? pl.ntasks - t0 : pl.gram_chunk;
     g.task_base = (int)t0; g.ntasks = (int)nt;
-    gram_kernel<T><<<dim3(tiles_x * g.tiles_y, (unsigned)nt), 256, 0, st>>>(g);
-    KSIG_CUDA(cudaGetLastError());
-    g_launches.fetch_add(1, std::memory_order_relaxed);
+    const dim3 ggrid(tiles_x * g.tiles_y, (unsigned)nt);
+    if constexpr (std::is_same<T, float>::value) {
+      if (tc) {
+        void* gargs[] = {&g};
+        KSIG_CUDA(launch_main((const void*)&gram_tc_kernel, ggrid, dim3(128), gargs,
+                              gram_tc_smem_bytes(), st));
+      } else {
+        gram_kernel<T><<<ggrid, 256, 0, st>>>(g);
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+      }
+    } else {
+      gram_kernel<T><<<ggrid, 256, 0, st>>>(g);
+      g_launches.fetch_add(1, std::memory_order_relaxed);
+    }
     a.task_base = (int)t0; a.ntasks = (int)nt;
     const long long blocks = (nt + pl.k->wpb - 1) / pl.k->wpb;
     const int grid = blocks < pl.grid ? (int)blocks : pl.grid;

@@ -65,6 +65,10 @@ struct SweepArgs {
   long long gram_slot;   // elements per slot
   int gram_ld;           // row stride of a slot
   int task_base, ntasks_total;
+  // Lane 0 leads the skewed sweep: each step it reads a grid row no lane
+  // has touched yet.  With x_prefetch > 0 it also prefetches (L1) the row
+  // x_prefetch steps ahead, so that its loads hit L1 like the other lanes'.
+  int x_prefetch;
 };
 
 // Item geometry a policy may need.
@@ -184,10 +188,24 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
       const int c0 = it.s * STRIP + C * lane;
 #pragma unroll
       for (int c = 0; c < C; ++c) xv[c] = __ldg(p + (c0 + c < it.Ly - 1 ? c0 + c : it.Ly - 1));
+      // Every lane reads fresh slot memory each step (its own columns of a
+      // new row): prefetch the row x_prefetch steps ahead into L2.
+      if (args.x_prefetch > 0) {
+        const int pr = row + args.x_prefetch < it.Lx - 1 ? row + args.x_prefetch : it.Lx - 1;
+        const int pc = c0 < it.Ly - 1 ? c0 : it.Ly - 1;
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(it.xb + (long long)pr * args.gram_ld + pc));
+      }
     } else {
       const V* p = reinterpret_cast<const V*>(it.xb + (long long)row * RS);
 #pragma unroll
       for (int v = 0; v < RS / VN; ++v) reinterpret_cast<V*>(xv)[v] = __ldg(p + v);
+      if (lane == 0 && args.x_prefetch > 0) {
+        const int pr = row + args.x_prefetch < it.Lx - 1 ? row + args.x_prefetch : it.Lx - 1;
+        const T* q = it.xb + (long long)pr * RS;
+#pragma unroll
+        for (int v = 0; v < (RS * (int)sizeof(T) + 127) / 128; ++v)
+          asm volatile("prefetch.global.L1 [%0];" ::"l"(q + v * (128 / sizeof(T))));
+      }
     }
   };
   // Static-kernel values of one grid row; call sites pass a literal for RBF,

@@ -114,11 +114,23 @@ def _to_seqs(X, n_features, reset_obj=None):
            else torch.zeros((1, d), dtype=dtype, device='cuda') for s in seqs],
           batch_first=True)
       return E.Seqs(padded.detach().contiguous(), lengths), False, padded
-    data = torch.zeros((len(seqs), Lmax, d), dtype=dtype, device='cuda')
-    for i, s in enumerate(seqs):
-      if s.shape[0] > 0:
-        data[i, :s.shape[0]] = s.to(device='cuda', dtype=dtype)
-    return E.Seqs(data, lengths), False, None
+    if all(not s.is_cuda for s in seqs):
+      # Host sequences: padded on the host, one host-to-device copy.
+      host = np.zeros((len(seqs), Lmax, d),
+                      dtype=np.float64 if dtype == torch.float64 else np.float32)
+      for i, s in enumerate(seqs):
+        if s.shape[0] > 0:
+          host[i, :s.shape[0]] = s.detach().numpy()
+      data = torch.from_numpy(host).to('cuda', non_blocking=False)
+    else:
+      # Device sequences: one padding kernel, no per-sequence copies.
+      data = torch.nn.utils.rnn.pad_sequence(
+          [s.to(device='cuda', dtype=dtype) if s.shape[0] > 0
+           else torch.zeros((1, d), dtype=dtype, device='cuda') for s in seqs],
+          batch_first=True)
+      if data.shape[1] < Lmax:
+        data = torch.nn.functional.pad(data, (0, 0, 0, Lmax - data.shape[1]))
+    return E.Seqs(data.contiguous(), lengths), False, None
   was_torch = isinstance(X, torch.Tensor)
   if not was_torch:
     X = torch.as_tensor(np.asarray(X))

@@ -120,3 +120,25 @@ def test_coverage_gradients(dt, tol, n_levels, order, d):
       lambda x, y: OT.signature_kernel(x, y, n_levels=n_levels, order=order,
                                        normalize=True, param=bw),
       X, Y, dt, tol)
+
+
+@pytest.mark.parametrize('tc', ['1', '0'])
+@pytest.mark.parametrize('d', [9, 16, 64])
+def test_gram_input_forms_match_oracle(tc, d, monkeypatch):
+  """The Gram-input sweep with the tensor-core (tcgen05, 3xTF32) or the
+  CUDA-core Gram tiles, forced at widths where a register tile exists too
+  (KSIG_FORCE_GIN), on random walks of 200 points (FP32, 1e-5)."""
+  import ksig_b200 as K
+  monkeypatch.setenv('KSIG_FORCE_GIN', '1')
+  monkeypatch.setenv('KSIG_GRAM_TC', tc)
+  rng = np.random.default_rng(d + 100)
+  inc = rng.standard_normal((6, 199, d)) / np.sqrt(200)
+  X = np.concatenate([np.zeros((6, 1, d)), np.cumsum(inc, 1)], 1).astype(np.float32)
+  inc = rng.standard_normal((5, 179, d)) / np.sqrt(180)
+  Y = np.concatenate([np.zeros((5, 1, d)), np.cumsum(inc, 1)], 1).astype(np.float32)
+  bw = float(np.sqrt(d))
+  k = K.SignatureKernel(n_levels=5, order=1, normalize=True, static_kernel=K.RBFKernel(bw))
+  ref = O.signature_kernel(X.astype(np.float64), Y.astype(np.float64), n_levels=5, param=bw)
+  assert _rel(k(X, Y), ref) < 1e-5
+  refx = O.signature_kernel(X.astype(np.float64), None, n_levels=5, param=bw)
+  assert _rel(k(X), refx) < 1e-5
