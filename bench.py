@@ -658,7 +658,9 @@ def run_gram_forms(args):
       ts.append(a.elapsed_time(b))
     return min(ts)
 
-  for dw in (8, 15, 31, 63):
+  dws = [int(v) - 1 for v in args.gram_d.split(',')] if args.gram_d else (8, 15, 31, 63)
+  forms = args.gram_forms.split(',') if args.gram_forms else ('register', 'tensor', 'cuda')
+  for dw in dws:
     d = dw + 1
     bw = math.sqrt(dw)
     X = torch.as_tensor(make_walks(n, SEQ_LEN, dw, 11), device=dev)
@@ -670,6 +672,8 @@ def run_gram_forms(args):
     row = {}
     for form, env in (('register', {}), ('tensor', {'KSIG_FORCE_GIN': '1', 'KSIG_GRAM_TC': '1'}),
                       ('cuda', {'KSIG_FORCE_GIN': '1', 'KSIG_GRAM_TC': '0'})):
+      if form not in forms:
+        continue
       if form == 'register' and d > 32:
         row[form] = {'unavailable': 'no register-Gram tile above 32 coordinates'}
         continue
@@ -935,6 +939,10 @@ def main():
                   help='dp512: the bench line; ragged-dp: the 2048 x 2048 ragged '
                        'order-2 workload, printed as its own report line')
   ap.add_argument('--plain-sample', type=int, default=96)
+  ap.add_argument('--gram-d', default=None,
+                  help='gram-forms: comma-separated channel counts (with time)')
+  ap.add_argument('--gram-forms', default=None,
+                  help='gram-forms: comma-separated subset of register,tensor,cuda')
   ap.add_argument('--n-seq', type=int, default=None,
                   help='sequences per side; smaller values are for profiling '
                        'captures only, not bench lines')

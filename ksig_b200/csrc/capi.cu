@@ -601,10 +601,11 @@ struct BwdPlan {
   long long scratch_per_warp;
   size_t off_scratch, total;
   long long rec_per_pair;  // split pass: record elements kept per pair
+  int ckpt;                // strip checkpointing (dp_bwd.cuh, DpBwdArgs::ckpt)
 };
 
 int plan_bwd(int nX, int LX, int nY, int LY, int d, int dtype, int n_levels, int order,
-             int difference, int pairs_mode, int n_list, BwdPlan& bp) {
+             int difference, int pairs_mode, int n_list, BwdPlan& bp, bool allow_ckpt = true) {
   int rc = plan_fwd(false, nX, LX, nY, LY, d, dtype, n_levels, order, difference, pairs_mode,
                     n_list, bp.f);
   if (rc) return rc;
@@ -657,9 +658,23 @@ int plan_bwd(int nX, int LX, int nY, int LY, int d, int dtype, int n_levels, int
   bp.rec_per_pair = ((long long)bp.ns_max * (bp.rows_max + 33) * bp.nx * 32 +
                      (long long)bp.ns_max * bp.nx * bp.c * 32 + 3) / 4 * 4;
   // The per-step records grow with the strip count and the row count; keep
-  // the whole scratch within a bounded budget by running fewer warps.
+  // the whole scratch within a bounded budget.  When the records of every
+  // strip would cap the warps below half of what the SMs hold, the adjoint
+  // keeps one strip of records and recomputes each strip's from its
+  // checkpoint (KSIG_DP_BWD_CKPT: 1 always for multi-strip shapes, 0 never,
+  // unset: that rule).  Recomputing costs a second forward pass over those
+  // strips: on the 2048-pair ragged order-2 sample (L up to 1024) the
+  // workspace fell from 32 GB to 3.3 GB and the adjoint rose 18 % on B200,
+  // so a mildly capped grid keeps the full records.
   const long long budget = (long long)env_int("KSIG_DP_BWD_SCRATCH_MB", 32768) << 20;
-  const long long cap = budget / (long long)(bp.scratch_per_warp * es);
+  long long cap = budget / (long long)(bp.scratch_per_warp * es);
+  bp.ckpt = 0;
+  const int ck_env = env_int("KSIG_DP_BWD_CKPT", -1);
+  if (allow_ckpt && bp.ns_max > 1 && (ck_env == 1 || (ck_env < 0 && 2 * cap < warps))) {
+    bp.ckpt = 1;
+    bp.scratch_per_warp = dp_bwd_scratch_elems(bp.ns_max, bp.rows_max, bp.nx, bp.c, 1);
+    cap = budget / (long long)(bp.scratch_per_warp * es);
+  }
   if (warps > cap) warps = cap > (long long)k->wpb ? cap : k->wpb;
   bp.grid = (int)((warps + k->wpb - 1) / k->wpb);
   bp.off_scratch = bp.f.off_scratch;  // the forward scratch region is unused here
@@ -721,6 +736,7 @@ int run_bwd(const BwdPlan& bp, const void* X, const int32_t* lenX, int nX, int L
   a.rows_max = bp.rows_max;
   a.status = status;
   a.phases = phases;
+  a.ckpt = bp.ckpt;
   if (phases != 3) {  // split pass: records per pair, after the plan's regions
     a.rec = reinterpret_cast<T*>(ws + bp.total);
     a.rec_per_pair = bp.rec_per_pair;
@@ -1442,7 +1458,8 @@ static int rec_plan(int nX, int LX, int nY, int LY, int d, int dtype, int n_leve
                     int difference, int pairs_mode, int n_list, BwdPlan& bp, size_t& total) {
   if (pairs_mode != KSIG_PAIRS_FULL && pairs_mode != KSIG_PAIRS_LIST)
     return fail(KSIG_ERR_UNSUPPORTED, "the split gradient pass takes full or listed pairs");
-  int rc = plan_bwd(nX, LX, nY, LY, d, dtype, n_levels, order, difference, pairs_mode, n_list, bp);
+  int rc = plan_bwd(nX, LX, nY, LY, d, dtype, n_levels, order, difference, pairs_mode, n_list, bp,
+                    false);
   if (rc) return rc;
   if (bp.f.p != 1 || n_levels < 2)
     return fail(KSIG_ERR_UNSUPPORTED, "the split gradient pass needs order 1 and n_levels >= 2");

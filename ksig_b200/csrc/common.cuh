@@ -139,37 +139,20 @@ __device__ __forceinline__ void rbf_center_col(YA& y, const CA& c0, T alpha) {
 }
 
 // Grid row x (raw) -> x' = x + negc (negc = column slot 0) with the norm
-// slot -a |x'|^2; xt may alias x.  FP32 pairs coordinates (FADD2 / FFMA2).
+// slot -a |x'|^2; xt may alias x.  Scalar FADD / FFMA: the paired forms
+// (FADD2 / FFMA2) were 5 % slower in the 512 x 512 sweep on B200, which
+// spent the saved issue slots on register moves to form the pairs.
 template <int KD, typename XA, typename NA>
 __device__ __forceinline__ void rbf_center_row(const XA& x, const NA& negc, float alpha,
                                                float* xt) {
-  if constexpr (KD >= 4) {
-    float2 n2 = make_float2(0.f, 0.f);
+  float n = 0.f;
 #pragma unroll
-    for (int j = 0; j < KD / 2; ++j) {
-      const float2 v = __fadd2_rn(make_float2(x[2 * j], x[2 * j + 1]),
-                                  make_float2(negc[2 * j], negc[2 * j + 1]));
-      xt[2 * j] = v.x;
-      xt[2 * j + 1] = v.y;
-      n2 = __ffma2_rn(v, v, n2);
-    }
-    float n = n2.x + n2.y;
-    if constexpr (KD % 2 == 1) {
-      const float v = x[KD - 1] + negc[KD - 1];
-      xt[KD - 1] = v;
-      n = fmaf(v, v, n);
-    }
-    xt[KD] = -alpha * n;
-  } else {
-    float n = 0.f;
-#pragma unroll
-    for (int k = 0; k < KD; ++k) {
-      const float v = x[k] + negc[k];
-      xt[k] = v;
-      n = fmaf(v, v, n);
-    }
-    xt[KD] = -alpha * n;
+  for (int k = 0; k < KD; ++k) {
+    const float v = x[k] + negc[k];
+    xt[k] = v;
+    n = fmaf(v, v, n);
   }
+  xt[KD] = -alpha * n;
 }
 template <int KD, typename XA, typename NA>
 __device__ __forceinline__ void rbf_center_row(const XA& x, const NA& negc, double alpha,

@@ -73,6 +73,12 @@ struct DpBwdArgs {
   // one launch.  `rec`: records per pair (rec_per_pair elements each) instead
   // of per warp.
   int phases;
+  // Strip checkpointing (one-launch adjoint of multi-strip pairs): phase 1
+  // keeps every strip's left-boundary stream and final column sums but the
+  // per-step records of the last strip only; phase 2 recomputes each other
+  // strip's records from its checkpoint just before its adjoint.  The
+  // records then need one strip of scratch instead of ns_max.
+  int ckpt;
   T* rec;
   long long rec_per_pair;
   double* lev;
@@ -80,13 +86,15 @@ struct DpBwdArgs {
 
 // Scratch elements per warp:
 //   REC [ns_max][rows_max + 33][NX][32]  phase-1 incoming prefixes per step
+//                                        ([1][...] with strip checkpointing)
 //   CS  [ns_max][NX][C][32]              final column sums per strip
 //   BL  [2][rows_max][NX]                forward strip-to-strip carries
+//                                        ([ns_max][...] with checkpointing)
 //   BR  [2][rows_max][NX]                adjoint strip-to-strip carries
 __host__ __device__ inline long long dp_bwd_scratch_elems(int ns_max, int rows_max, int nx,
-                                                          int c) {
-  return (long long)ns_max * (rows_max + 33) * nx * 32 + (long long)ns_max * nx * c * 32 +
-         4LL * rows_max * nx;
+                                                          int c, int ckpt = 0) {
+  return (long long)(ckpt ? 1 : ns_max) * (rows_max + 33) * nx * 32 +
+         (long long)ns_max * nx * c * 32 + (long long)(ckpt ? ns_max + 2 : 4) * rows_max * nx;
 }
 
 // Dynamic shared memory per block: each lane keeps its C + 1 packed column
@@ -112,8 +120,13 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
   // Two steps per loop trip remove the per-step register moves of the
   // pipelined row state.  FP32 order 1 only: the order >= 2 and FP64
   // instances hold more state per cell, and there the unrolled loop spills
-  // more and runs slower.
+  // more and runs slower.  The adjoint pass (phase 2) of the 7-column tiles
+  // runs one step per trip since the lane-centred Gram raised its state:
+  // unrolled it spilled 920 bytes at d = 9, and one step per trip took the
+  // 512 x 512 adjoint from 86.5 to 78.5 ms and the replayed pass from 65.7
+  // to 52.4 ms on B200.
   constexpr int kStepUnroll = (sizeof(T) == 4 && P == 1) ? 2 : 1;
+  constexpr int kStepUnroll2 = (sizeof(T) == 4 && P == 1 && C < 7) ? 2 : 1;
   // Paired FP32 Gram arguments (packed_arg) where they keep the occupancy.
   constexpr bool kPairArg = sizeof(T) == 4 && KD <= 16 && (C >= 7 || P >= 2);
 
@@ -126,10 +139,11 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
   T* scr = args.scratch + wg * args.scratch_per_warp;
   const long long steps_max = (long long)args.rows_max + 33;
   const long long rm = args.rows_max;
-  const long long cs_off = (long long)args.ns_max * steps_max * NX * 32;
+  const int ckpt = args.ckpt && !args.rec;  // per-pair records keep every strip
+  const long long cs_off = (long long)(ckpt ? 1 : args.ns_max) * steps_max * NX * 32;
   T* const REC0 = scr;
   T* BL = REC0 + cs_off + (long long)args.ns_max * NX * C * 32;
-  T* BR = BL + 2 * rm * NX;
+  T* BR = BL + (long long)(ckpt ? args.ns_max : 2) * rm * NX;
   const int phases = FWD_ONLY ? 1 : (args.phases ? args.phases : 3);
 
   const double alpha = 1.4426950408889634 / fmax(2.0 * args.param * args.param, 1e-12);
@@ -237,7 +251,11 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
         }
       }
     };
-    auto rec_at = [&](int s, long long t) { return REC + ((long long)s * steps_max + t) * NX * 32; };
+    auto rec_at = [&](int s, long long t) {
+      return REC + ((long long)(ckpt ? 0 : s) * steps_max + t) * NX * 32;
+    };
+    // Forward carries of strip s (its lane 31's exchange values per row).
+    auto bl_at = [&](int s) { return BL + (long long)(ckpt ? s : (s & 1)) * rm * NX; };
 
     T Ccol[NX][C];  // forward column sums (rows above the current row)
     // Forward-only launches: per-lane level totals (FP64), levels 1..NL.
@@ -246,7 +264,10 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
     for (int k = 0; k <= NL; ++k) lt[k] = 0.0;
 
     // ---------------- phase 1: forward, top-down, strips left to right -----
-    for (int s = 0; s < ((phases & 1) ? ns : 0); ++s) {
+    // One strip of the forward pass: records (rec_on), carries to the next
+    // strip and final column sums (cs_on).  Phase 2 calls it again for the
+    // strips whose records were not kept (strip checkpointing).
+    auto fwd_strip = [&](int s, bool rec_on, bool cs_on) {
       stage_y(s);
 #pragma unroll
       for (int h = 0; h < NX; ++h)
@@ -260,8 +281,8 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
       for (int c = 0; c < C; ++c) { Mprev[c] = T(0); DMold[c] = T(0); }
       T xc[RS];
       load_x(-lane, xc);
-      const T* blin = BL + (long long)((s + 1) & 1) * rm * NX;  // written by strip s - 1
-      T* blout = BL + (long long)(s & 1) * rm * NX;
+      const T* blin = bl_at(s > 0 ? s - 1 : 1);  // written by strip s - 1 (read when s > 0)
+      T* blout = bl_at(s);
       const int T1 = lx + 33;
 #pragma unroll kStepUnroll
       for (int t = 0; t < T1; ++t) {
@@ -291,7 +312,7 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
 #pragma unroll
         for (int c = 0; c < C; ++c)
           if (!act || s * STRIP + C * lane + c >= ly) Z[c] = T(0);
-        if (act && NH > 0) {
+        if (rec_on && act && NH > 0) {
           T* rp = rec_at(s, t);
 #pragma unroll
           for (int h = 0; h < NX; ++h) rp[h * 32 + lane] = Xin[h];
@@ -393,7 +414,7 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
       }
       // Final column sums: read back by the adjoint pass (the last strip's
       // stay in registers when both passes run in one launch).
-      if ((ns > 1 && s + 1 < ns) || !(phases & 2)) {
+      if (cs_on && ((ns > 1 && s + 1 < ns) || !(phases & 2))) {
         T* dst = CS + (long long)s * NX * C * 32;
 #pragma unroll
         for (int h = 0; h < NX; ++h)
@@ -401,7 +422,8 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
           for (int c = 0; c < C; ++c) dst[(h * C + c) * 32 + lane] = Ccol[h][c];
       }
       __syncwarp();  // carries and records of this strip -> later readers
-    }
+    };
+    for (int s = 0; s < ((phases & 1) ? ns : 0); ++s) fwd_strip(s, !ckpt || s == ns - 1, true);
     if constexpr (FWD_ONLY) {
       // Level totals of the pair: lanes summed in a fixed order (FP64).
 #pragma unroll
@@ -415,6 +437,7 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
 
     // ---------------- phase 2: adjoint, bottom-up, strips right to left ----
     for (int s = (phases & 2) ? ns - 1 : -1; s >= 0; --s) {
+      if (ckpt && s != ns - 1) fwd_strip(s, true, false);  // this strip's records
       stage_y(s);
       if (s != ns - 1 || !(phases & 1)) {
         const T* src = CS + (long long)s * NX * C * 32;
@@ -452,7 +475,7 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
           recn[h] = (act0 && NH > 0) ? rec_at(s, lx + 33)[h * 32 + lane] : T(0);
       }
       const int T2 = lx + 33;
-#pragma unroll kStepUnroll
+#pragma unroll kStepUnroll2
       for (int u = 0; u < T2; ++u) {
         const int rho = u - (31 - lane);
         const int g = lx - rho;                      // grid row computed; cell row processed

@@ -65,9 +65,8 @@ struct SweepArgs {
   long long gram_slot;   // elements per slot
   int gram_ld;           // row stride of a slot
   int task_base, ntasks_total;
-  // Lane 0 leads the skewed sweep: each step it reads a grid row no lane
-  // has touched yet.  With x_prefetch > 0 it also prefetches (L1) the row
-  // x_prefetch steps ahead, so that its loads hit L1 like the other lanes'.
+  // Gram input: every lane reads a new slot row each step; with
+  // x_prefetch > 0 it prefetches (L2) the row x_prefetch steps ahead.
   int x_prefetch;
 };
 
@@ -199,13 +198,6 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
       const V* p = reinterpret_cast<const V*>(it.xb + (long long)row * RS);
 #pragma unroll
       for (int v = 0; v < RS / VN; ++v) reinterpret_cast<V*>(xv)[v] = __ldg(p + v);
-      if (lane == 0 && args.x_prefetch > 0) {
-        const int pr = row + args.x_prefetch < it.Lx - 1 ? row + args.x_prefetch : it.Lx - 1;
-        const T* q = it.xb + (long long)pr * RS;
-#pragma unroll
-        for (int v = 0; v < (RS * (int)sizeof(T) + 127) / 128; ++v)
-          asm volatile("prefetch.global.L1 [%0];" ::"l"(q + v * (128 / sizeof(T))));
-      }
     }
   };
   // Static-kernel values of one grid row; call sites pass a literal for RBF,
