@@ -163,6 +163,8 @@ def instances():
       add(('pde', dt, 0, 2, 0, f, 0))
     for c in ([2, 4, 8] if dt == 'f32' else [2]):
       add(('ga', dt, 0, c, 0, 1, 0))
+  # The adjoint with strip checkpointing: one per adjoint tile.
+  out += [('dpc',) + inst[1:] for inst in out if inst[0] == 'dpb']
   # Forward pass of the split gradient pass: one per order-1 adjoint tile
   # with at least two levels (same tile, same records).
   out += [('dpr',) + inst[1:] for inst in out
@@ -178,13 +180,14 @@ OPS = {
     'ga': ('OP_GA_FWD', 'ga_fwd_kernel<{T}, {kd}, {c}, {wpb}>'),
     'dpb': ('OP_DP_BWD', 'dp_bwd_kernel<{T}, {kd}, {c}, {nl}, {p}, {wpb}>'),
     'dpr': ('OP_DP_REC_FWD', 'dp_rec_fwd_kernel<{T}, {kd}, {c}, {nl}, {p}, {wpb}>'),
+    'dpc': ('OP_DP_BWD_CKPT', 'dp_bwd_ckpt_kernel<{T}, {kd}, {c}, {nl}, {p}, {wpb}>'),
     'pdeb': ('OP_PDE_BWD', 'pde_bwd_kernel<{T}, {kd}, {c}, {p}, {wpb}>'),
 }
 
 
 HEADER = {'dp': 'sweep.cuh', 'pde': 'sweep.cuh', 'dpx': 'sweep.cuh',
           'pdex': 'sweep.cuh', 'ga': 'sweep.cuh', 'dpb': 'dp_bwd.cuh',
-          'dpr': 'dp_bwd.cuh', 'pdeb': 'pde_bwd.cuh'}
+          'dpr': 'dp_bwd.cuh', 'dpc': 'dp_bwd.cuh', 'pdeb': 'pde_bwd.cuh'}
 
 
 def _group_key(inst):

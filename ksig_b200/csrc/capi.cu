@@ -549,12 +549,14 @@ int run_fwd(const FwdPlan& pl, const void* X, const int32_t* lenX, int nX, int L
   g.slot = pl.gram_slot; g.ld = pl.gram_ld;
   // The CUDA-core difference tiles (gram.cuh) by default; RBF in FP32 with
   // KSIG_GRAM_TC=1: the tensor-core tiles (gram_tc.cuh).  The tensor-core
-  // form centres once per 32 columns and carries 3xTF32 products, so it is
-  // less accurate than the difference tiles on widely spread paths, and the
-  // sweep's reads of the slots, not the Gram, bound this path's time.
+  // tiles are faster from 128 coordinates (B200, 128 x 128 pairs, L = 200:
+  // 15.1 vs 16.8 ms at d = 128, 25.7 vs 31.2 ms at d = 256), but with one
+  // centre per 32 columns and 3xTF32 products they missed the 1e-5 bar on
+  // widely spread paths (d = 64 and d = 160 walks with steps of 0.2 per
+  // channel), where the difference tiles do not cancel.
   bool tc = false;
   if constexpr (std::is_same<T, float>::value)
-    tc = kind == KIND_RBF && env_int("KSIG_GRAM_TC", 0) != 0;
+    tc = kind == KIND_RBF && env_int("KSIG_GRAM_TC", 0) > 0;
   const int tm = tc ? kTcM : kGramTile, tn = tc ? kTcN : kGramTile;
   const int tiles_x = (pl.gram_rows + tm - 1) / tm;
   g.tiles_y = (pl.gram_ld + tn - 1) / tn;
@@ -602,6 +604,7 @@ struct BwdPlan {
   size_t off_scratch, total;
   long long rec_per_pair;  // split pass: record elements kept per pair
   int ckpt;                // strip checkpointing (dp_bwd.cuh, DpBwdArgs::ckpt)
+  const KernelEntry* kc;   // its kernel (dp_bwd_ckpt_kernel), when ckpt
 };
 
 int plan_bwd(int nX, int LX, int nY, int LY, int d, int dtype, int n_levels, int order,
@@ -670,10 +673,23 @@ int plan_bwd(int nX, int LX, int nY, int LY, int d, int dtype, int n_levels, int
   long long cap = budget / (long long)(bp.scratch_per_warp * es);
   bp.ckpt = 0;
   const int ck_env = env_int("KSIG_DP_BWD_CKPT", -1);
+  bp.kc = nullptr;
   if (allow_ckpt && bp.ns_max > 1 && (ck_env == 1 || (ck_env < 0 && 2 * cap < warps))) {
-    bp.ckpt = 1;
-    bp.scratch_per_warp = dp_bwd_scratch_elems(bp.ns_max, bp.rows_max, bp.nx, bp.c, 1);
-    cap = budget / (long long)(bp.scratch_per_warp * es);
+    const KernelEntry* kc =
+        find_kernel(OP_DP_BWD_CKPT, bp.f.f64, k->kd, bp.c, k->nl, bp.f.p, 1);
+    if (kc && kc->kd == k->kd && kc->c == bp.c && kc->nl == k->nl) {
+      e = ensure_smem_attr(kc->func, bp.dyn_smem);
+      if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(dp backward, checkpointed)");
+      int occc = 0;
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occc, kc->func, k->wpb * 32, bp.dyn_smem);
+      if (e != cudaSuccess || occc <= 0) occc = 1;
+      warps = (long long)sms * occc * k->wpb;
+      if (warps > bp.f.ntasks) warps = bp.f.ntasks > 0 ? bp.f.ntasks : 1;
+      bp.ckpt = 1;
+      bp.kc = kc;
+      bp.scratch_per_warp = dp_bwd_scratch_elems(bp.ns_max, bp.rows_max, bp.nx, bp.c, 1);
+      cap = budget / (long long)(bp.scratch_per_warp * es);
+    }
   }
   if (warps > cap) warps = cap > (long long)k->wpb ? cap : k->wpb;
   bp.grid = (int)((warps + k->wpb - 1) / k->wpb);
@@ -742,7 +758,7 @@ int run_bwd(const BwdPlan& bp, const void* X, const int32_t* lenX, int nX, int L
     a.rec_per_pair = bp.rec_per_pair;
   }
   a.lev = lev;
-  const void* func = bp.k->func;
+  const void* func = bp.ckpt && phases == 3 ? bp.kc->func : bp.k->func;
   if (phases == 1) {
     const KernelEntry* e = rec_fwd_entry(bp);
     if (!e) return fail(KSIG_ERR_UNSUPPORTED, "no compiled split forward pass for this tile");

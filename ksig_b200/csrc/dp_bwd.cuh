@@ -107,7 +107,8 @@ __host__ __device__ inline size_t dp_bwd_smem_bytes(int wpb, int c, int rs, size
 // Kernel body.  RBF_NOPAR: RBF static kernel and no parameter gradient,
 // known at compile time (no per-point kind tests, no distance arguments
 // kept for dparam).
-template <typename T, int KD, int C, int NL, int P, int WPB, bool RBF_NOPAR, bool FWD_ONLY>
+template <typename T, int KD, int C, int NL, int P, int WPB, bool RBF_NOPAR, bool FWD_ONLY,
+          bool CKPT = false>
 __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
   using Lay = DpLayout<NL, P>;
   constexpr int NH = Lay::NH;
@@ -123,8 +124,9 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
   // more and runs slower.  The adjoint pass (phase 2) of the 7-column tiles
   // runs one step per trip since the lane-centred Gram raised its state:
   // unrolled it spilled 920 bytes at d = 9, and one step per trip took the
-  // 512 x 512 adjoint from 86.5 to 78.5 ms and the replayed pass from 65.7
-  // to 52.4 ms on B200.
+  // 512 x 512 adjoint from 86.5 to 78 ms on B200.  Phase 1 keeps two steps
+  // per trip (one step: one-launch adjoint 78 -> 82 ms, forward-only pass
+  // 23 -> 35 ms).
   constexpr int kStepUnroll = (sizeof(T) == 4 && P == 1) ? 2 : 1;
   constexpr int kStepUnroll2 = (sizeof(T) == 4 && P == 1 && C < 7) ? 2 : 1;
   // Paired FP32 Gram arguments (packed_arg) where they keep the occupancy.
@@ -139,7 +141,9 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
   T* scr = args.scratch + wg * args.scratch_per_warp;
   const long long steps_max = (long long)args.rows_max + 33;
   const long long rm = args.rows_max;
-  const int ckpt = args.ckpt && !args.rec;  // per-pair records keep every strip
+  // Strip checkpointing is compiled into its own kernel (dp_bwd_ckpt_kernel),
+  // so that the recompute path does not weigh on the others' registers.
+  constexpr bool ckpt = CKPT;
   const long long cs_off = (long long)(ckpt ? 1 : args.ns_max) * steps_max * NX * 32;
   T* const REC0 = scr;
   T* BL = REC0 + cs_off + (long long)args.ns_max * NX * C * 32;
@@ -437,7 +441,9 @@ __device__ __forceinline__ void dp_bwd_body(const DpBwdArgs<T>& args) {
 
     // ---------------- phase 2: adjoint, bottom-up, strips right to left ----
     for (int s = (phases & 2) ? ns - 1 : -1; s >= 0; --s) {
-      if (ckpt && s != ns - 1) fwd_strip(s, true, false);  // this strip's records
+      if constexpr (CKPT) {
+        if (s != ns - 1) fwd_strip(s, true, false);  // this strip's records
+      }
       stage_y(s);
       if (s != ns - 1 || !(phases & 1)) {
         const T* src = CS + (long long)s * NX * C * 32;
@@ -823,6 +829,14 @@ dp_bwd_kernel(const DpBwdArgs<T> args) {
     dp_bwd_body<T, KD, C, NL, P, WPB, true, false>(args);
   else
     dp_bwd_body<T, KD, C, NL, P, WPB, false, false>(args);
+}
+
+// The adjoint with strip checkpointing (DpBwdArgs::ckpt): phase 1 keeps one
+// strip of records, phase 2 recomputes the others from their checkpoints.
+template <typename T, int KD, int C, int NL, int P, int WPB>
+__global__ void __launch_bounds__(WPB * 32)
+dp_bwd_ckpt_kernel(const DpBwdArgs<T> args) {
+  dp_bwd_body<T, KD, C, NL, P, WPB, false, false, true>(args);
 }
 
 // Forward pass of the split gradient pass (order 1): phase 1 with per-pair

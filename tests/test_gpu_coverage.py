@@ -142,3 +142,23 @@ def test_gram_input_forms_match_oracle(tc, d, monkeypatch):
   assert _rel(k(X, Y), ref) < 1e-5
   refx = O.signature_kernel(X.astype(np.float64), None, n_levels=5, param=bw)
   assert _rel(k(X), refx) < 1e-5
+
+
+@pytest.mark.parametrize('d', [128, 160])
+def test_wide_spread_walks(d):
+  """Widely spread walks (steps of 0.2 per channel) at 128 and 160
+  coordinates through the default Gram-input path (CUDA-core difference
+  tiles), FP32 against the FP64 oracle at 1e-5, normalised and not."""
+  import ksig_b200 as K
+  rng = np.random.default_rng(d + 7)
+  X = _walks(rng, 4, 45, d).astype(np.float32)
+  Y = _walks(rng, 3, 38, d).astype(np.float32)
+  bw = float(np.sqrt(d) * 0.5)
+  X64, Y64 = X.astype(np.float64), Y.astype(np.float64)
+  for normalize, order, m in ((True, 1, 5), (False, 2, 4)):
+    k = K.SignatureKernel(n_levels=m, order=order, normalize=normalize,
+                          static_kernel=K.RBFKernel(bw))
+    assert _rel(k(X, Y), O.signature_kernel(X64, Y64, n_levels=m, order=order,
+                                            normalize=normalize, param=bw)) < 1e-5
+    assert _rel(k(X), O.signature_kernel(X64, None, n_levels=m, order=order,
+                                         normalize=normalize, param=bw)) < 1e-5
