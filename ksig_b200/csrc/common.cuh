@@ -102,6 +102,20 @@ __device__ __forceinline__ double packed_arg(const XA& x, const YA& y, double) {
 // small), unlike |x|^2 + |y|^2 - 2 <x, y> for long unnormalised paths, where
 // both norms reach 1e4 in FP32.  Column 0 needs no dot product at all.
 
+// Pairwise sum of N values (a balanced tree: rounding error grows with
+// log2 N, not N).
+template <int N, typename T>
+__device__ __forceinline__ T pair_sum(const T (&v)[N]) {
+  T s[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) s[i] = v[i];
+#pragma unroll
+  for (int w = 1; w < N; w *= 2)
+#pragma unroll
+    for (int i = 0; i + w < N; i += 2 * w) s[i] += s[i + w];
+  return s[0];
+}
+
 // Raw column points y[c][0..KD] (slot KD zero) -> lane-centred form; slot 0
 // is the centre.  NC columns in a [NC][KD + 1] array.
 template <int KD, int NC, typename T>

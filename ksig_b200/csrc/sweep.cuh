@@ -68,6 +68,13 @@ struct SweepArgs {
   // Gram input: every lane reads a new slot row each step; with
   // x_prefetch > 0 it prefetches (L2) the row x_prefetch steps ahead.
   int x_prefetch;
+  // Visiting order.  0: warp w takes task positions w, w + W, w + 2W, ...
+  // (W warps in the grid).  > 0 (FULL pairs, no task permutation): warp w
+  // takes the visit_per consecutive entries w * visit_per, ... of the
+  // column-major pair order (b = p / nX, a = p % nX), so consecutive pairs
+  // of a warp share their column sequence and the lanes keep their column
+  // points across the switch.
+  long long visit_per;
 };
 
 // Item geometry a policy may need.
@@ -84,9 +91,22 @@ struct SweepSmem {
   T ynext[32][C * RS];
 };
 
+// Per-warp ring of item descriptors.  Every lane of a warp visits the same
+// items in the same order, lane 0 first (the other lanes follow 1..31 steps
+// behind), so lane 0 decodes each new pair once and leaves its geometry
+// here; the other lanes copy it when they reach that pair.  Items span at
+// least 16 row steps, so lane 31 trails lane 0 by at most 2 items, well
+// inside the ring.
+template <typename T>
+struct ItemMeta {
+  const T* xb;
+  int task, b, Lx, Ly, rows, ns;
+};
+constexpr int kItemRing = 8;
+
 template <typename T, int KD, int C, bool DIFF, int WPB, bool EXT, class Policy>
 __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
-                                      SweepSmem<T, KD, C>& sm) {
+                                      SweepSmem<T, KD, C>& sm, ItemMeta<T>* ring) {
   constexpr int NX = Policy::NX;
   // KD == 0: Gram input.  The per-step "x row" of a lane is then its C
   // static-kernel values of that grid row, read from the task's Gram slot.
@@ -112,15 +132,31 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
   auto make_item = [&](long long q, Item& it) {
     it.seq = q;
     it.s = 0;
-    const long long tid = wg + q * nw;
+    long long tid;
+    int2 ab;
+    if (!GIN && args.visit_per > 0) {
+      // Column-major block of this warp (FULL pairs, natural task order).
+      const long long p = wg * args.visit_per + q;
+      tid = (q < args.visit_per && p < args.ntasks) ? p : args.ntasks;
+      if (tid < args.ntasks) {  // p < ntasks fits an int
+        const int pi = (int)p;
+        const int b = pi / args.nX;
+        ab = make_int2(pi - b * args.nX, b);
+        it.task = ab.x * args.nY + ab.y;
+      }
+    } else {
+      tid = wg + q * nw;
+      if (tid < args.ntasks) {
+        const int pos = args.task_base + (int)tid;
+        it.task = args.order ? args.order[pos] : pos;
+        ab = decode_task(pos, args.mode, args.nY, args.list, args.order);
+      }
+    }
     if (tid >= args.ntasks) {
       it.task = -1; it.b = 0; it.Lx = 1; it.Ly = 1; it.rows = 16; it.ns = 1;
       it.xb = GIN ? args.gram : args.xr;
       return;
     }
-    const int pos = args.task_base + (int)tid;
-    it.task = args.order ? args.order[pos] : pos;
-    int2 ab = decode_task(pos, args.mode, args.nY, args.list, args.order);
     if (ab.x < 0 || ab.x >= args.nX || ab.y < 0 || ab.y >= args.nYseq) {
       set_status(args.status, KSIG_ERR_INVALID);  // pair index out of range
       ab = make_int2(0, 0);
@@ -135,18 +171,40 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
     it.rows = lx > 16 ? lx : 16;
     if (it.ns > 1 && it.rows < 32) it.rows = 32;
   };
-  auto next_of = [&](const Item& cur, Item& nx) {
+  // from_ring: called in a lane's own item switch (divergent), where lane 0
+  // decodes the pair and the others copy its descriptor (ItemMeta).
+  auto next_of = [&](const Item& cur, Item& nx, bool from_ring) {
     if (cur.task >= 0 && cur.s + 1 < cur.ns) {
       nx = cur;
       nx.s = cur.s + 1;
+      return;
+    }
+    const long long q = cur.seq + 1;
+    if (!from_ring) {
+      make_item(q, nx);
+      return;
+    }
+    ItemMeta<T>& m = ring[q & (kItemRing - 1)];
+    if (lane == 0) {
+      make_item(q, nx);
+      m.xb = nx.xb; m.task = nx.task; m.b = nx.b; m.Lx = nx.Lx; m.Ly = nx.Ly;
+      m.rows = nx.rows; m.ns = nx.ns;
     } else {
-      make_item(cur.seq + 1, nx);
+      nx.seq = q; nx.s = 0;
+      nx.xb = m.xb; nx.task = m.task; nx.b = m.b; nx.Lx = m.Lx; nx.Ly = m.Ly;
+      nx.rows = m.rows; nx.ns = m.ns;
     }
   };
   auto ycol_ptr = [&](const Item& it, int c) {
     int col = it.s * STRIP + C * lane + c;
     col = col < it.Ly - 1 ? col : it.Ly - 1;
     return args.yr + (args.ystart[it.b] + col) * RS;
+  };
+  // Two items with the same column sequence and strip give every lane the
+  // same column points (the column-major visiting order makes this the
+  // common case): the switch between them keeps the lane's registers.
+  auto same_y = [&](const Item& p, const Item& n) {
+    return !GIN && p.task >= 0 && n.task >= 0 && p.b == n.b && p.s == n.s;
   };
   // Stages the lane's column points of `it` into its smem slot.
   auto stage_y = [&](const Item& it) {
@@ -250,7 +308,7 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
 
   Item cur, nxt;
   make_item(0, cur);
-  next_of(cur, nxt);
+  next_of(cur, nxt, false);
   // First item's columns straight into registers; the next item is staged.
   if (!GIN && cur.task >= 0) {
 #pragma unroll
@@ -269,7 +327,7 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
 #pragma unroll
       for (int k = 0; k <= KD; ++k) yv[c][k] = T(0);
   }
-  stage_y(nxt);
+  if (!same_y(cur, nxt)) stage_y(nxt);
 
   const bool rbf = args.kind == KIND_RBF;
   // Gram input serves every static kind through the steady loop.
@@ -434,7 +492,7 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
 
     // Rare, uniform branches: item switches.
     if (__any_sync(FULL, active && last_row)) {
-      if (active && last_row && nxt.task >= 0) y_from_slot();
+      if (active && last_row && nxt.task >= 0 && !same_y(cur, nxt)) y_from_slot();
     }
     if (__any_sync(FULL, pv && pr == 0)) {
       if (pv && pr == 0) {
@@ -480,15 +538,19 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
     }
     // Item switch of the position (rare, uniform).
     if (__any_sync(FULL, (active && last_row) || (rec && u == 2))) {
-      if (rec && u == 2) pit = cur;          // first recorded row of cur
+      // pit: the item of the recorded rows, from cur's first recorded row
+      // on (it still names cur when cur's last row runs, after the switch).
+      if (rec && u == 2) pit = cur;
       if (active && last_row) {
-        pit = cur;                           // last row recorded for cur
         cur = nxt;
-        next_of(cur, nxt);
+        next_of(cur, nxt, true);
         if (cur.task < 0) done = true;
-        else stage_y(nxt);
+        else if (!same_y(cur, nxt)) stage_y(nxt);
         u = 0;
       }
+      // Orders lane 0's ring entry (next_of) before the other lanes read it
+      // at their own switches, one or more steps later.
+      __syncwarp();
     }
     // Prefetch the x row of the next step's Gram.
     {
@@ -693,19 +755,15 @@ struct DpPolicy {
     for (int h = 0; h < NX; ++h) X[h] = H[h];
   }
 
-  // Folds a finished strip's column totals into the lane's level totals.
+  // Folds a finished strip's column totals into the lane's level totals: the
+  // lane's C column sums of a level are added pairwise in T (depth
+  // ceil(log2 C)), the sum once converted and accumulated in FP64.  Lanes
+  // reach this at different steps, so it runs for one lane at a time; the
+  // short form keeps that serial part small.
   __device__ void end_item() {
 #pragma unroll
-    for (int k = 1; k < NL; ++k) {
-      double s = 0.0;
-#pragma unroll
-      for (int c = 0; c < C; ++c) s += (double)Ccol[L::off(k + 1)][c];
-      accd[k] += s;
-    }
-    double s = 0.0;
-#pragma unroll
-    for (int c = 0; c < C; ++c) s += (double)Clast[c];
-    accd[NL] += s;
+    for (int k = 1; k < NL; ++k) accd[k] += (double)pair_sum<C>(Ccol[L::off(k + 1)]);
+    accd[NL] += (double)pair_sum<C>(Clast);
   }
 
   __device__ void end_task(long long seq, int, int lane) {
@@ -734,12 +792,13 @@ struct DpPolicy {
 template <typename T, int KD, int C, int NL, int P, bool DIFF, int WPB, bool EXT>
 __global__ void __launch_bounds__(WPB * 32)
 dp_fwd_kernel(const SweepArgs<T> args) {
+  __shared__ ItemMeta<T> ring[WPB][kItemRing];
   __shared__ double red[WPB][2][NL][32];
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   auto* sm = reinterpret_cast<SweepSmem<T, KD, C>*>(dyn_smem);
   DpPolicy<T, C, NL, P, WPB> pol;
   pol.init(red[threadIdx.x >> 5], args.out, args.ntasks_total, args.nl_out);
-  sweep<T, KD, C, DIFF, WPB, EXT>(args, pol, sm[threadIdx.x >> 5]);
+  sweep<T, KD, C, DIFF, WPB, EXT>(args, pol, sm[threadIdx.x >> 5], ring[threadIdx.x >> 5]);
 }
 
 // ---------------------------------------------------------------------------
@@ -856,11 +915,12 @@ struct PdePolicy {
 template <typename T, int KD, int C, int F, bool DIFF, int WPB, bool EXT>
 __global__ void __launch_bounds__(WPB * 32)
 pde_fwd_kernel(const SweepArgs<T> args) {
+  __shared__ ItemMeta<T> ring[WPB][kItemRing];
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   auto* sm = reinterpret_cast<SweepSmem<T, KD, C>*>(dyn_smem);
   PdePolicy<T, C, F, DIFF> pol;
   pol.init(args.out);
-  sweep<T, KD, C, DIFF, WPB, EXT>(args, pol, sm[threadIdx.x >> 5]);
+  sweep<T, KD, C, DIFF, WPB, EXT>(args, pol, sm[threadIdx.x >> 5], ring[threadIdx.x >> 5]);
 }
 
 // ---------------------------------------------------------------------------
@@ -950,11 +1010,12 @@ struct GaPolicy {
 template <typename T, int KD, int C, int WPB>
 __global__ void __launch_bounds__(WPB * 32)
 ga_fwd_kernel(const SweepArgs<T> args) {
+  __shared__ ItemMeta<T> ring[WPB][kItemRing];
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   auto* sm = reinterpret_cast<SweepSmem<T, KD, C>*>(dyn_smem);
   GaPolicy<T, C> pol;
   pol.init(args.out);
-  sweep<T, KD, C, false, WPB, false>(args, pol, sm[threadIdx.x >> 5]);
+  sweep<T, KD, C, false, WPB, false>(args, pol, sm[threadIdx.x >> 5], ring[threadIdx.x >> 5]);
 }
 
 }  // namespace ksig
