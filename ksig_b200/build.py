@@ -30,12 +30,13 @@ LIB = os.path.join(LIB_DIR, 'libksig_b200.so')
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 NVCC_FLAGS = ['-O3', '-std=c++17', '-Xcompiler', '-fPIC',
               '-Xcompiler', '-O2', '--expt-relaxed-constexpr', '-ftz=true']
-# Line info (source correlation for ncu) on the FP32 forward units and the
-# C ABI; the FP64 and adjoint units are built without it to keep the library
-# small.
+# Line info (source correlation for ncu) on the C ABI and the FP32 order-1
+# DP forward units (the profiled sweeps); the other units are built without
+# it, which keeps the library about half its size (line info makes a unit's
+# object 3.7 times larger).
 def _wants_lineinfo(src):
   name = os.path.basename(src)
-  return name == 'capi.cu' or name.startswith(('inst_dp_f32', 'inst_pde_f32'))
+  return name == 'capi.cu' or name.startswith('inst_dp_f32_p1_d1_')
 WPB = 2  # warps per block of the sweep kernels
 
 KD_ALL = [2, 4, 6, 8, 9, 10, 12, 16, 24, 32]

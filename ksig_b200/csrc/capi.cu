@@ -164,6 +164,7 @@ double rbf_alpha(int kind, double param) {
 
 // Workspace carve-up shared by the forward kernels.
 struct FwdPlan {
+  int family;             // 0 DP, 1 PDE, 2 global alignment
   int f64, kd, rs, c, nl, nl_out, p, diff, nx_exchange;
   long long ntasks;
   int multi, grid, wpb;
@@ -339,6 +340,7 @@ int plan_fwd(int family, int nX, int LX, int nY, int LY, int d, int dtype, int n
              FwdPlan& pl, bool allow_order = true, bool ext = false,
              bool layout_only = false) {
   const bool pde = family == 1, ga = family == 2;
+  pl.family = family;
   if (dtype != KSIG_DTYPE_F32 && dtype != KSIG_DTYPE_F64)
     return fail(KSIG_ERR_INVALID, "dtype must be KSIG_DTYPE_F32 or KSIG_DTYPE_F64");
   if (nX <= 0 || LX <= 0 || d <= 0) return fail(KSIG_ERR_INVALID, "empty X (n=%d, L=%d, d=%d)", nX, LX, d);
@@ -534,6 +536,22 @@ int run_fwd(const FwdPlan& pl, const void* X, const int32_t* lenX, int nX, int L
       env_int("KSIG_VISIT", 1) > 0) {
     const long long nw = (long long)pl.grid * pl.k->wpb;
     a.visit_per = (pl.ntasks + nw - 1) / nw;
+  }
+  // Stacked pairs (SweepArgs::stack_len): the DP levels of one column's
+  // pairs in a warp's block run as one item, the separator rows between
+  // the stacked row sequences folding each pair (one item switch per
+  // column instead of per pair).  An item switch costs the warp about 35
+  // steps at three times the cost of a plain step, the stacked form a few
+  // instructions per step: B200, 512 columns of L = 200, d = 9, m = 5:
+  // 512 rows of L = 200 20.7 -> 16.7 ms, 256 of L = 400 17.7 -> 16.2 ms,
+  // 64 of L = 1600 15.5 -> 16.0 ms; hence row sequences up to 1024 points.
+  // KSIG_STACK=0 switches it off, KSIG_STACK=1 on for any length.
+  a.stack_len = 0;
+  {
+    const int st = env_int("KSIG_STACK", -1);
+    if (a.visit_per > 0 && pl.family == 0 && pl.diff && !pl.multi && LX >= 17 &&
+        (st > 0 || (st < 0 && LX <= 1024)))
+      a.stack_len = LX;
   }
   a.kind = kind;
   a.sp = sp;

@@ -75,6 +75,13 @@ struct SweepArgs {
   // of a warp share their column sequence and the lanes keep their column
   // points across the switch.
   long long visit_per;
+  // > 0 (with visit_per, DP policies, differencing, one strip per pair, row
+  // sequences of stack_len >= 17 points each): the pairs of one column in a
+  // warp's block run as one item of stacked row sequences.  The cell row
+  // between two stacked sequences gets Z = 0, and each lane folds the level
+  // totals of the pair above it and clears its state there (fold_pair), so
+  // the pairs in between need no item switch.
+  int stack_len;
 };
 
 // Item geometry a policy may need.
@@ -116,6 +123,11 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
   using V = typename Vec<T>::type;
   constexpr int STRIP = DIFF ? 32 * C - 1 : 32 * C;
   constexpr bool kPairArg = Policy::kPairArg && KD <= 16;
+  // Stacking needs a few registers per lane (nb, nf, pbnd): only tiles of
+  // up to 12 coordinates, where they fit without spilling (d = 32, 2
+  // columns, m = 10 went from 0 to 210 bytes of spills with them).
+  constexpr bool kStackable = DIFF && !GIN && Policy::kStack && KD <= 12;
+  const bool stack_on = kStackable && args.stack_len > 0 && args.visit_per > 0;
 
   const int lane = threadIdx.x & 31;
   const long long wg = (long long)blockIdx.x * WPB + (threadIdx.x >> 5);
@@ -123,7 +135,8 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
   T* bbuf = args.scratch ? args.scratch + wg * args.scratch_per_warp : nullptr;
   T* yslot = sm.ynext[lane];
 
-  // One item = one strip of one pair.
+  // One item = one strip of one pair, or Lx / stack_len stacked pairs of
+  // one column (task is then the first pair's, the others follow nY apart).
   struct Item {
     const T* xb;  // first packed row of the row sequence
     long long seq;
@@ -132,9 +145,26 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
   auto make_item = [&](long long q, Item& it) {
     it.seq = q;
     it.s = 0;
+    int np = 1;  // stacked pairs
     long long tid;
     int2 ab;
-    if (!GIN && args.visit_per > 0) {
+    if (stack_on) {
+      // Run q of this warp's block: the pairs of its q-th column.
+      const long long p0 = wg * args.visit_per;
+      long long pend = p0 + args.visit_per;
+      if (pend > args.ntasks) pend = args.ntasks;
+      const long long b0 = p0 / args.nX;
+      const long long start = q == 0 ? p0 : (b0 + q) * args.nX;
+      long long end = (b0 + q + 1) * args.nX;
+      if (end > pend) end = pend;
+      tid = start < end ? start : args.ntasks;
+      if (tid < args.ntasks) {
+        const int b = (int)(start / args.nX);
+        ab = make_int2((int)(start - (long long)b * args.nX), b);
+        it.task = ab.x * args.nY + ab.y;
+        np = (int)(end - start);
+      }
+    } else if (!GIN && args.visit_per > 0) {
       // Column-major block of this warp (FULL pairs, natural task order).
       const long long p = wg * args.visit_per + q;
       tid = (q < args.visit_per && p < args.ntasks) ? p : args.ntasks;
@@ -163,7 +193,7 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
     }
     it.b = ab.y;
     it.xb = GIN ? args.gram + tid * args.gram_slot : args.xr + args.xstart[ab.x] * RS;
-    it.Lx = args.xlen[ab.x];
+    it.Lx = np > 1 ? np * args.stack_len : args.xlen[ab.x];
     it.Ly = args.ylen[ab.y];
     const int lx = DIFF ? it.Lx - 1 : it.Lx;
     const int ly = DIFF ? it.Ly - 1 : it.Ly;
@@ -354,6 +384,15 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
   int u = 0;
   int delay = lane;
   bool done = cur.task < 0;
+  // Stacked pairs: nb is the step position whose recorded row is the next
+  // separator of cur; pbnd marks the recorded row as one; nf counts this
+  // lane's finished pairs (the reduction slot parity, the same sequence in
+  // every lane).  The pair of a recorded row pr of a stacked item is
+  // (pr + 1) / stack_len.
+  constexpr int kNoBound = 0x7fffffff;
+  int nb = (stack_on && cur.Lx > args.stack_len) ? args.stack_len : kNoBound;
+  bool pbnd = false;
+  unsigned nf = 0;
 
   // Cells of the recorded row + Gram of the next grid row (into Mn, with
   // vertical differences DMn against Mc).  `pvf` is false only when nothing
@@ -374,7 +413,23 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
     }
     // Lane 31's last cell belongs to the next strip when differencing.
     const bool mask_last = DIFF && lane == 31;
+    if constexpr (kStackable) {
+      // The recorded row separates two stacked pairs (its Z is zero): the
+      // state holds the upper pair's final column sums.
+      if (pbnd) {
+        pol.fold_pair(nf, lane);
+        ++nf;
+      }
+    }
     pol.row(pZ, Xin, mask_last, pvf, pr, ItemInfo{pit.task, pit.Lx, pit.Ly, pit.s, pit.ns}, lane);
+    if constexpr (kStackable) {
+      // A stacked pair is complete once lane 31 has folded it.
+      if (stack_on && __shfl_sync(FULL, pbnd ? 1 : 0, 31)) {
+        const long long q = __shfl_sync(FULL, nf, 31) - 1;
+        const int t = __shfl_sync(FULL, pit.task + ((pr + 1) / args.stack_len - 1) * args.nY, 31);
+        pol.collect(q, t, lane);
+      }
+    }
     if (lane == 31 && pvf && pit.s + 1 < pit.ns) {
       T* dst = bbuf + (long long)pr * NX;
 #pragma unroll
@@ -395,6 +450,16 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
 #pragma unroll
       for (int c = 0; c < C - 1; ++c) pZ[c] = rec ? DMc[c + 1] - DMc[c] : T(0);
       pZ[C - 1] = (rec && lane != 31) ? DMright - DMc[C - 1] : T(0);
+      if constexpr (kStackable) {
+        // Cell row u-1 lies between two stacked sequences (grid rows
+        // j*stack_len - 1 and j*stack_len): no cell, Z = 0.
+        pbnd = rec && u == nb;
+        if (pbnd) {
+          nb += args.stack_len;
+#pragma unroll
+          for (int c = 0; c < C; ++c) pZ[c] = T(0);
+        }
+      }
     } else {
       const int g0 = cur.s * STRIP + C * lane;
 #pragma unroll
@@ -513,16 +578,20 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
       if (fin_item) {
         pol.end_item();
         if (pit.s + 1 >= pit.ns) {
-          pol.end_task(pit.seq, pit.task, lane);
+          pol.end_task(kStackable ? (long long)nf : pit.seq, pit.task, lane);
           fin = true;
         }
       }
-      // A pair is complete once lane 31 (the last lane) has finished it.
+      // A pair is complete once lane 31 (the last lane) has finished it (of
+      // a stacked item, the last pair, (pr + 1) / stack_len).
       if (__shfl_sync(FULL, fin ? 1 : 0, 31)) {
-        const long long q = __shfl_sync(FULL, pit.seq, 31);
-        const int t = __shfl_sync(FULL, pit.task, 31);
+        const long long q = kStackable ? (long long)__shfl_sync(FULL, nf, 31)
+                                       : __shfl_sync(FULL, pit.seq, 31);
+        const int last = stack_on ? (pr + 1) / args.stack_len : 0;
+        const int t = __shfl_sync(FULL, pit.task + last * args.nY, 31);
         pol.collect(q, t, lane);
       }
+      if (kStackable && fin) ++nf;
     }
 
     // Record cell row u-1 for the next step, advance.
@@ -547,6 +616,7 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
         if (cur.task < 0) done = true;
         else if (!same_y(cur, nxt)) stage_y(nxt);
         u = 0;
+        nb = (stack_on && cur.Lx > args.stack_len) ? args.stack_len : kNoBound;
       }
       // Orders lane 0's ring entry (next_of) before the other lanes read it
       // at their own switches, one or more steps later.
@@ -601,6 +671,10 @@ struct DpPolicy {
   // truncations and the 4-column higher-order tiles, where the register
   // count and occupancy stay the same.
   static constexpr bool kPairArg = sizeof(T) == 4 && NL >= 5 && (C >= 7 || (P >= 2 && C >= 4));
+  // Stacked pairs (SweepArgs::stack_len) end with fold_pair.  Order 1
+  // only: the order-p state leaves no registers for the stacking counters
+  // (d = 16, 4 columns, m = 8, p = 2 spilled 116 bytes with them).
+  static constexpr bool kStack = P == 1;
   T X[NX];                    // horizontal running sums (outgoing)
   T Ccol[NX][C];              // column running sums
   T Clast[C];                 // column sums of the last level's totals
@@ -634,10 +708,15 @@ struct DpPolicy {
   // apart from X, which no active neighbour reads then.
   __device__ void row(const T (&Z)[C], const T (&Xin)[NX], bool, bool, int,
                       const ItemInfo&, int) {
-    if (P == 1) {
+    if constexpr (P == 1) {
       row_order1(Z, Xin);
-      return;
+    } else {
+      row_order_p(Z, Xin);
     }
+  }
+
+  // Order p >= 2 (Alg. 6).
+  __device__ void row_order_p(const T (&Z)[C], const T (&Xin)[NX]) {
     T H[NX];
 #pragma unroll
     for (int h = 0; h < NX; ++h) H[h] = Xin[h];
@@ -766,6 +845,14 @@ struct DpPolicy {
     accd[NL] += (double)pair_sum<C>(Clast);
   }
 
+  // End of a stacked pair at its separator row: fold and publish its level
+  // totals (reduction slot `slot`), clear the state for the next pair.
+  __device__ void fold_pair(long long slot, int lane) {
+    end_item();
+    end_task(slot, 0, lane);
+    begin_item();
+  }
+
   __device__ void end_task(long long seq, int, int lane) {
 #pragma unroll
     for (int k = 1; k <= NL; ++k) {
@@ -821,6 +908,7 @@ struct PdePolicy {
   static constexpr int NX = 2 * F;
   static constexpr bool kUnroll2 = C * F <= 16 && sizeof(T) == 4;
   static constexpr bool kPairArg = false;
+  static constexpr bool kStack = false;
   static constexpr int STRIP = DIFF ? 32 * C - 1 : 32 * C;
   T X[NX];
   T Kr[C * F];
@@ -952,6 +1040,7 @@ struct GaPolicy {
   static constexpr int NX = 1;
   static constexpr bool kUnroll2 = false;
   static constexpr bool kPairArg = false;
+  static constexpr bool kStack = false;
   static constexpr int STRIP = 32 * C;
   T X[NX];
   T Kr[C];       // logK of the row above, the lane's columns

@@ -1,0 +1,58 @@
+"""Visiting orders of the forward sweep on full pair grids.
+
+Equal-length full grids run in column-major blocks per warp, and the DP
+levels of one column's pairs in a block run stacked as one item (separator
+rows between the row sequences fold each pair).  Each pair is computed by
+one warp with the same arithmetic whatever the order, so the per-level
+results must be bit-identical to the round-robin order without stacking.
+The grids are large enough that every warp gets pairs from more than one
+column, and short enough (17 points) to reach the smallest stacked length.
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle import ksig_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _walks(rng, n, L, d):
+  inc = rng.standard_normal((n, L - 1, d)) / np.sqrt(L)
+  return np.concatenate([np.zeros((n, 1, d)), np.cumsum(inc, 1)], 1)
+
+
+def _levels(X, Y, n_levels, order, monkeypatch, stack, visit):
+  from ksig_b200 import _engine as E
+  from ksig_b200 import _lib as L
+  monkeypatch.setenv('KSIG_STACK', stack)
+  monkeypatch.setenv('KSIG_VISIT', visit)
+  return E.sig_levels(E.Seqs(X), E.Seqs(Y), L.PAIRS_FULL, n_levels, order, True,
+                      L.STATIC_RBF, 0.9)
+
+
+@pytest.mark.parametrize('dt', [torch.float32, torch.float64])
+@pytest.mark.parametrize('order,n_levels,nx,lx,ny,ly', [
+    (1, 5, 300, 17, 77, 50),
+    (1, 3, 131, 33, 97, 120),
+    (2, 4, 260, 24, 45, 70),
+    (1, 4, 1000, 40, 3, 60),
+])
+def test_stacked_pairs_bit_identical(dt, order, n_levels, nx, lx, ny, ly, monkeypatch):
+  rng = np.random.default_rng(nx + lx + order)
+  X = torch.tensor(_walks(rng, nx, lx, 3), dtype=dt, device='cuda')
+  Y = torch.tensor(_walks(rng, ny, ly, 3), dtype=dt, device='cuda')
+  ref = _levels(X, Y, n_levels, order, monkeypatch, '0', '0')
+  blocks = _levels(X, Y, n_levels, order, monkeypatch, '0', '1')
+  stacked = _levels(X, Y, n_levels, order, monkeypatch, '1', '1')
+  assert torch.equal(blocks, ref)
+  assert torch.equal(stacked, ref)
+  # A few pairs against the oracle (the stacked rows of neighbouring pairs
+  # must not leak into each other).
+  Xn, Yn = X.double().cpu().numpy(), Y.double().cpu().numpy()
+  for a, b in ((0, 0), (nx - 1, ny - 1), (nx // 2, ny // 3)):
+    want = O.signature_kernel(Xn[a:a + 1], Yn[b:b + 1], n_levels=n_levels, order=order,
+                              normalize=False, param=0.9)[0, 0]
+    got = float(stacked[:, a * ny + b].sum())
+    tol = 1e-5 if dt == torch.float32 else 1e-11
+    assert abs(got - want) <= tol * abs(want)
