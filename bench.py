@@ -369,6 +369,7 @@ def run_ours(args, rank, world, dist):
   # Forward + backward (gradient of sum(W * K) w.r.t. X through the adjoint
   # kernels), the 'fwd+bwd s/step' half of the metric.
   fb_ms = None
+  fb_steps_ms = None
   split_used = None
   if not args.no_bwd:
     Xg = Xd.clone().requires_grad_(True)
@@ -380,9 +381,10 @@ def run_ours(args, rank, world, dist):
       (Kg * Wt).sum().backward()
       return Xg.grad
 
-    for _ in range(2):
+    for _ in range(3):
       fb_step()
     barrier()
+    rec0 = dict(E.REC_STATS)
     fbs = []
     for i in range(args.bwd_steps):
       flush.fill_(i & 0xff)
@@ -394,9 +396,10 @@ def run_ours(args, rank, world, dist):
       b.synchronize()
       fbs.append(a.elapsed_time(b))
     fb_ms = sum(fbs) / len(fbs)
-    # Whether the split gradient pass ran (its workspace is pooled after a
-    # backward) rather than the sweep plus the one-launch adjoint.
-    split_used = bool(E._REC_POOL.get(torch.cuda.current_device()))
+    fb_steps_ms = [round(v, 3) for v in fbs]
+    # Timed steps whose forward kept the split gradient pass's records (the
+    # backward replays them) and those that ran the one-launch adjoint.
+    split_used = {k: E.REC_STATS[k] - rec0[k] for k in rec0}
     if dist is not None:
       t = torch.tensor([fb_ms], device=dev, dtype=torch.float64)
       dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -461,6 +464,7 @@ def run_ours(args, rank, world, dist):
             's_per_step': fb_ms * 1e-3, 'ms_per_step': fb_ms,
             'what': 'K(X, Y) forward + dL/dX backward (L = sum W*K), '
                     'X [512, 200, 9] requires grad', 'steps': args.bwd_steps,
+            'step_ms': fb_steps_ms,
             'split_pass': split_used},
         'gpu_launches': int(launches),
         'clocks': clk,

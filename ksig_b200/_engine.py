@@ -198,6 +198,10 @@ def sig_levels_bwd(X, Y, mode, n_levels, order, kind, param, grad_levels,
 # cannot overwrite records the adjoint is still reading.  The pool holds at
 # most KSIG_REC_MB bytes per device.
 _REC_POOL = {}
+# Forwards that kept the split pass's records, and those that declined them
+# (no compiled split pass, or records above rec_budget_bytes): a backward
+# after a declined forward runs the one-launch adjoint.
+REC_STATS = {'recorded': 0, 'declined': 0}
 
 
 def _dev_index(device):
@@ -262,7 +266,9 @@ def sig_levels_rec(X, Y, n_levels, order, kind, param, pair_list=None):
   ws_bytes = lib.ksig_signature_kern_rec_workspace(
       X.n, X.L, Y.n, Y.L, X.d, dt, n_levels, order, 1, mode, n_list)
   if ws_bytes == 0 or ws_bytes > rec_budget_bytes(X.data.device):
+    REC_STATS['declined'] += 1
     return None
+  REC_STATS['recorded'] += 1
   P = num_pairs(mode, X.n, Y.n, n_list)
   out = torch.empty((n_levels + 1, max(P, 0)), dtype=torch.float64,
                     device=X.data.device)
