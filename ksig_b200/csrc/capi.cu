@@ -525,15 +525,16 @@ int run_fwd(const FwdPlan& pl, const void* X, const int32_t* lenX, int nX, int L
   // register-Gram sweeps gained nothing from it.
   a.x_prefetch = env_int("KSIG_XPF", pl.gin ? 4 : 0);
   // Column-major blocks per warp (sweep.cuh, SweepArgs::visit_per) where the
-  // pairs are a full grid of equal-length sequences: consecutive pairs of a
+  // pairs are a full grid or the upper triangle of K(X) over equal-length
+  // sequences: consecutive pairs of a
   // warp then share their column sequence, a pair switch reloads no column
   // points, and every warp gets the same number of equal pairs (512 x 512
   // pairs, L = 200, d = 9, m = 5 on a B200: 24.4 -> 23.3 ms).  Ragged grids
   // keep the round-robin order over the longest-first permutation.
   // KSIG_VISIT=0 keeps the round-robin order (measurement).
   a.visit_per = 0;
-  if (!pl.gin && mode == KSIG_PAIRS_FULL && !a.order && !lenX && !lenY &&
-      env_int("KSIG_VISIT", 1) > 0) {
+  if (!pl.gin && (mode == KSIG_PAIRS_FULL || mode == KSIG_PAIRS_UPPER) && !a.order && !lenX &&
+      !lenY && env_int("KSIG_VISIT", 1) > 0) {
     const long long nw = (long long)pl.grid * pl.k->wpb;
     a.visit_per = (pl.ntasks + nw - 1) / nw;
   }
@@ -549,7 +550,8 @@ int run_fwd(const FwdPlan& pl, const void* X, const int32_t* lenX, int nX, int L
   a.stack_len = 0;
   {
     const int st = env_int("KSIG_STACK", -1);
-    if (a.visit_per > 0 && pl.family == 0 && pl.diff && !pl.multi && LX >= 17 &&
+    if (a.visit_per > 0 && mode == KSIG_PAIRS_FULL && pl.family == 0 && pl.diff && !pl.multi &&
+        LX >= 17 &&
         (st > 0 || (st < 0 && LX <= 1024)))
       a.stack_len = LX;
   }

@@ -69,10 +69,11 @@ struct SweepArgs {
   // x_prefetch > 0 it prefetches (L2) the row x_prefetch steps ahead.
   int x_prefetch;
   // Visiting order.  0: warp w takes task positions w, w + W, w + 2W, ...
-  // (W warps in the grid).  > 0 (FULL pairs, no task permutation): warp w
-  // takes the visit_per consecutive entries w * visit_per, ... of the
-  // column-major pair order (b = p / nX, a = p % nX), so consecutive pairs
-  // of a warp share their column sequence and the lanes keep their column
+  // (W warps in the grid).  > 0 (FULL or UPPER pairs, no task
+  // permutation): warp w takes the visit_per consecutive entries
+  // w * visit_per, ... of the column-major pair order (column b: rows
+  // 0 .. nX-1, or 0 .. b of the upper triangle), so consecutive pairs of a
+  // warp share their column sequence and the lanes keep their column
   // points across the switch.
   long long visit_per;
   // > 0 (with visit_per, DP policies, differencing, one strip per pair, row
@@ -142,6 +143,21 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
     long long seq;
     int task, b, Lx, Ly, rows, ns, s;
   };
+  // Upper triangle of K(X) in column-major order: column b holds rows
+  // 0 .. b, from position b (b + 1) / 2 on.  tri_col inverts that; the
+  // output slot of pair (a, b) is its row-major position upper_task.
+  const bool upper = args.mode == KSIG_PAIRS_UPPER;
+  auto tri_col = [&](long long p) {
+    long long b = (long long)((sqrt(8.0 * (double)p + 1.0) - 1.0) * 0.5);
+    if (b < 0) b = 0;
+    while (b > 0 && b * (b + 1) / 2 > p) --b;
+    while ((b + 1) * (b + 2) / 2 <= p) ++b;
+    return b;
+  };
+  auto upper_task = [&](long long a, long long b) {
+    return (int)(a * args.nY - a * (a - 1) / 2 + (b - a));
+  };
+
   auto make_item = [&](long long q, Item& it) {
     it.seq = q;
     it.s = 0;
@@ -164,7 +180,7 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
         it.task = ab.x * args.nY + ab.y;
         np = (int)(end - start);
       }
-    } else if (!GIN && args.visit_per > 0) {
+    } else if (!GIN && args.visit_per > 0 && !upper) {
       // Column-major block of this warp (FULL pairs, natural task order).
       const long long p = wg * args.visit_per + q;
       tid = (q < args.visit_per && p < args.ntasks) ? p : args.ntasks;
@@ -173,6 +189,20 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
         const int b = pi / args.nX;
         ab = make_int2(pi - b * args.nX, b);
         it.task = ab.x * args.nY + ab.y;
+      }
+    } else if (!GIN && args.visit_per > 0) {
+      // Upper triangle: the q-th pair of this warp's column-major block
+      // (column b: rows 0 .. b).
+      const long long p0 = wg * args.visit_per;
+      long long pend = p0 + args.visit_per;
+      if (pend > args.ntasks) pend = args.ntasks;
+      const long long start = p0 + q;
+      tid = start < pend ? start : args.ntasks;
+      if (tid < args.ntasks) {
+        const long long b = tri_col(start);
+        const long long a = start - b * (b + 1) / 2;
+        ab = make_int2((int)a, (int)b);
+        it.task = upper_task(a, b);
       }
     } else {
       tid = wg + q * nw;
@@ -385,10 +415,9 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
   int delay = lane;
   bool done = cur.task < 0;
   // Stacked pairs: nb is the step position whose recorded row is the next
-  // separator of cur; pbnd marks the recorded row as one; nf counts this
-  // lane's finished pairs (the reduction slot parity, the same sequence in
-  // every lane).  The pair of a recorded row pr of a stacked item is
-  // (pr + 1) / stack_len.
+  // separator of cur; nf counts this lane's finished pairs (the reduction
+  // slot parity, the same sequence in every lane).  The pair of a recorded
+  // row r of a stacked item is (r + 1) / stack_len.
   constexpr int kNoBound = 0x7fffffff;
   int nb = (stack_on && cur.Lx > args.stack_len) ? args.stack_len : kNoBound;
   bool pbnd = false;
@@ -399,6 +428,22 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
   // was recorded (pZ is zero then).
   auto main_block = [&](int rbf_c, bool pvf, const T (&Mc)[C], T (&Mn)[C], T (&DMn)[C],
                         T& DMright) {
+    if constexpr (kStackable) {
+      // The recorded row separates two stacked pairs (its Z is zero); the
+      // state holds the upper pair's final column sums: fold them and
+      // clear the state.  A stacked pair is complete once lane 31 has
+      // folded it.  Both branches come first in the step, ahead of the
+      // Gram and the recursion, which stay one block for the scheduler.
+      if (pbnd) {
+        pol.fold_pair(nf, lane);
+        ++nf;
+      }
+      if (stack_on && __shfl_sync(FULL, pbnd ? 1 : 0, 31)) {
+        const long long q = (long long)__shfl_sync(FULL, nf, 31) - 1;
+        const int t = __shfl_sync(FULL, pit.task + ((pr + 1) / args.stack_len - 1) * args.nY, 31);
+        pol.collect(q, t, lane);
+      }
+    }
     T Xin[NX];
 #pragma unroll
     for (int h = 0; h < NX; ++h) Xin[h] = shfl_up(pol.X[h], 1);
@@ -413,23 +458,7 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
     }
     // Lane 31's last cell belongs to the next strip when differencing.
     const bool mask_last = DIFF && lane == 31;
-    if constexpr (kStackable) {
-      // The recorded row separates two stacked pairs (its Z is zero): the
-      // state holds the upper pair's final column sums.
-      if (pbnd) {
-        pol.fold_pair(nf, lane);
-        ++nf;
-      }
-    }
     pol.row(pZ, Xin, mask_last, pvf, pr, ItemInfo{pit.task, pit.Lx, pit.Ly, pit.s, pit.ns}, lane);
-    if constexpr (kStackable) {
-      // A stacked pair is complete once lane 31 has folded it.
-      if (stack_on && __shfl_sync(FULL, pbnd ? 1 : 0, 31)) {
-        const long long q = __shfl_sync(FULL, nf, 31) - 1;
-        const int t = __shfl_sync(FULL, pit.task + ((pr + 1) / args.stack_len - 1) * args.nY, 31);
-        pol.collect(q, t, lane);
-      }
-    }
     if (lane == 31 && pvf && pit.s + 1 < pit.ns) {
       T* dst = bbuf + (long long)pr * NX;
 #pragma unroll

@@ -1,8 +1,9 @@
 """Visiting orders of the forward sweep on full pair grids.
 
-Equal-length full grids run in column-major blocks per warp, and the DP
-levels of one column's pairs in a block run stacked as one item (separator
-rows between the row sequences fold each pair).  Each pair is computed by
+Equal-length full grids and K(X) upper triangles run in column-major blocks
+per warp, and on full grids the DP levels of one column's pairs in a block
+run stacked as one item (separator rows between the row sequences fold each
+pair).  Each pair is computed by
 one warp with the same arithmetic whatever the order, so the per-level
 results must be bit-identical to the round-robin order without stacking.
 The grids are large enough that every warp gets pairs from more than one
@@ -54,5 +55,36 @@ def test_stacked_pairs_bit_identical(dt, order, n_levels, nx, lx, ny, ly, monkey
     want = O.signature_kernel(Xn[a:a + 1], Yn[b:b + 1], n_levels=n_levels, order=order,
                               normalize=False, param=0.9)[0, 0]
     got = float(stacked[:, a * ny + b].sum())
+    tol = 1e-5 if dt == torch.float32 else 1e-11
+    assert abs(got - want) <= tol * abs(want)
+
+
+@pytest.mark.parametrize('dt', [torch.float32, torch.float64])
+@pytest.mark.parametrize('n,lx,n_levels', [(300, 33, 5), (1000, 17, 4), (77, 50, 3), (5, 20, 5)])
+def test_stacked_upper_triangle_bit_identical(dt, n, lx, n_levels, monkeypatch):
+  """K(X): column-major blocks over the upper triangle (column b holds rows
+  0 .. b) against the round-robin order (KSIG_STACK=1 must leave the
+  triangle unstacked and unchanged); the output slots keep the row-major
+  upper-triangle order."""
+  from ksig_b200 import _engine as E
+  from ksig_b200 import _lib as L
+  rng = np.random.default_rng(n + lx)
+  X = torch.tensor(_walks(rng, n, lx, 3), dtype=dt, device='cuda')
+
+  def levels(stack, visit):
+    monkeypatch.setenv('KSIG_STACK', stack)
+    monkeypatch.setenv('KSIG_VISIT', visit)
+    return E.sig_levels(E.Seqs(X), None, L.PAIRS_UPPER, n_levels, 1, True, L.STATIC_RBF, 0.9)
+
+  ref = levels('0', '0')
+  assert torch.equal(levels('0', '1'), ref)
+  stacked = levels('1', '1')
+  assert torch.equal(stacked, ref)
+  Xn = X.double().cpu().numpy()
+  tot = stacked.sum(0).cpu().numpy()
+  for a, b in ((0, n - 1), (n // 2, n // 2), (n - 2, n - 1)):
+    want = O.signature_kernel(Xn[a:a + 1], Xn[b:b + 1], n_levels=n_levels, normalize=False,
+                              param=0.9)[0, 0]
+    got = tot[a * n - a * (a - 1) // 2 + (b - a)]
     tol = 1e-5 if dt == torch.float32 else 1e-11
     assert abs(got - want) <= tol * abs(want)
