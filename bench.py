@@ -465,6 +465,7 @@ def run_ours(args, rank, world, dist):
             'what': 'K(X, Y) forward + dL/dX backward (L = sum W*K), '
                     'X [512, 200, 9] requires grad', 'steps': args.bwd_steps,
             'step_ms': fb_steps_ms,
+            'median_ms': statistics.median(fb_steps_ms) if fb_steps_ms else None,
             'split_pass': split_used},
         'gpu_launches': int(launches),
         'clocks': clk,
@@ -937,7 +938,7 @@ def main():
   ap.add_argument('--no-plain', action='store_true')
   ap.add_argument('--no-ragged', action='store_true',
                   help='skip the ragged order-2 sub-record of the bench line')
-  ap.add_argument('--bwd-steps', type=int, default=5)
+  ap.add_argument('--bwd-steps', type=int, default=10)
   ap.add_argument('--workload', default='dp512',
                   choices=['dp512', 'ragged-dp', 'ragged-pde', 'mmd-pde', 'gram-forms'],
                   help='dp512: the bench line; ragged-dp: the 2048 x 2048 ragged '
