@@ -111,3 +111,31 @@ def test_stacked_pairs_other_static_kernels(static, monkeypatch):
   monkeypatch.setenv('KSIG_STACK', '1')
   monkeypatch.setenv('KSIG_VISIT', '1')
   assert np.array_equal(kern(X, Y), ref)
+
+
+def test_stacked_pairs_bench_size(monkeypatch):
+  """The bench workload at full size (512 x 512 pairs, L = 200, d = 8 + time,
+  m = 5, RBF): stacked, blocked and round-robin orders give the same levels
+  bit for bit, and sampled pairs match the FP64 oracle."""
+  import bench
+  X = torch.as_tensor(bench.make_walks(512, 200, 8, 2), device='cuda')
+  Y = torch.as_tensor(bench.make_walks(512, 200, 8, 3), device='cuda')
+  from ksig_b200 import _engine as E
+  from ksig_b200 import _lib as L
+
+  def levels(stack, visit):
+    monkeypatch.setenv('KSIG_STACK', stack)
+    monkeypatch.setenv('KSIG_VISIT', visit)
+    return E.sig_levels(E.Seqs(X), E.Seqs(Y), L.PAIRS_FULL, 5, 1, True, L.STATIC_RBF,
+                        float(np.sqrt(8)))
+
+  ref = levels('0', '0')
+  assert torch.equal(levels('0', '1'), ref)
+  stacked = levels('1', '1')
+  assert torch.equal(stacked, ref)
+  Xn, Yn = X.double().cpu().numpy(), Y.double().cpu().numpy()
+  for a, b in ((0, 0), (511, 511), (300, 17), (17, 300)):
+    want = O.signature_kernel(Xn[a:a + 1], Yn[b:b + 1], n_levels=5, normalize=False,
+                              param=float(np.sqrt(8)))[0, 0]
+    got = float(stacked[:, a * 512 + b].sum())
+    assert abs(got - want) <= 1e-5 * abs(want)
