@@ -307,7 +307,12 @@ int want_cols(int ly_cells, int cap, int op) {
   if (tuned > 0) return tuned;
   const int forced = env_int("KSIG_FWD_COLS", 0);
   if (forced > 0) return forced;
-  static const int opts[] = {2, 4, 7, 8};
+  // The PDE and global-alignment sweeps are compiled for 2, 4 and 8
+  // columns (8 up to 16 coordinates).  For the PDE the widest strip that
+  // covers a row in one pass wins: 512 x 512 pairs of L = 200 ran in
+  // 23.7 ms with 8 columns (one strip) against 27.8 ms with 4 (two strips),
+  // 33.1 against 37.9 ms at dyadic order 1 (caps per family in plan_fwd).
+  static const int opts[] = {2, 4, 8};
   if (op == OP_DP_FWD) {
     // Fewest lane-steps per row with a per-step overhead of 1.5 cells:
     // strips * (C + 1.5), ties to the wider strip.  Fitted to B200 timings
@@ -373,7 +378,13 @@ int plan_fwd(int family, int nX, int LX, int nY, int LY, int d, int dtype, int n
   const int lx_cells = pl.diff ? LX - 1 : LX;
   const int op = ga ? OP_GA_FWD
                    : ext ? (pde ? OP_PDE_FWD_EXT : OP_DP_FWD_EXT) : (pde ? OP_PDE_FWD : OP_DP_FWD);
-  const int want = want_cols(ly_cells, 8, op);
+  // Column caps measured on a B200 (256 x 256 pairs, L = 200, d = 9): the
+  // PDE gains from 8 columns up to dyadic order 2 (4.9 against 7.6 ms at
+  // order 0, 13.9 against 20.0 ms at order 2); order 3 (C * F = 64 refined
+  // values per lane) stays at 4; the global-alignment sweep (a log-sum-exp
+  // per cell) ran 21.4 ms with 4 columns and 33.8 ms with 8.
+  const int cap = ga ? 4 : (pde && p >= 8) ? 4 : 8;
+  const int want = want_cols(ly_cells, cap, op);
   // KSIG_FORCE_GIN=1 takes the Gram-input path even where a register-Gram
   // tile exists (measurement of the two Gram forms on the same shapes).
   const KernelEntry* k = (layout_only || env_int("KSIG_FORCE_GIN", 0))
@@ -538,23 +549,27 @@ int run_fwd(const FwdPlan& pl, const void* X, const int32_t* lenX, int nX, int L
     const long long nw = (long long)pl.grid * pl.k->wpb;
     a.visit_per = (pl.ntasks + nw - 1) / nw;
   }
-  // Stacked pairs (SweepArgs::stack_len): the DP levels of one column's
-  // pairs in a warp's block run as one item, the separator rows between
-  // the stacked row sequences folding each pair (one item switch per
-  // column instead of per pair).  An item switch costs the warp about 35
-  // steps at three times the cost of a plain step, the stacked form a few
-  // instructions per step: B200, 512 columns of L = 200, d = 9, m = 5:
-  // 512 rows of L = 200 20.7 -> 16.7 ms, 256 of L = 400 17.7 -> 16.2 ms,
-  // 64 of L = 1600 15.5 -> 16.0 ms; hence row sequences up to 1024 points.
-  // KSIG_STACK=0 switches it off, KSIG_STACK=1 on for any length.
+  // Stacked pairs (SweepArgs::stack_len): the pairs of one column in a
+  // warp's block run as one item, the separator rows between the stacked
+  // row sequences folding each pair (DP levels) or resetting the lane's K
+  // values (PDE), so a column needs one item switch instead of one per
+  // pair.  An item switch costs the warp about 35 steps at three times the
+  // cost of a plain step, the stacked form a few instructions per step.
+  // B200, 512 columns of L = 200, d = 9, DP m = 5: 512 rows of L = 200
+  // 20.7 -> 16.7 ms, 256 of L = 400 17.7 -> 16.2 ms, 64 of L = 1600
+  // 15.5 -> 16.0 ms; hence row sequences up to 1024 points.  KSIG_STACK=0
+  // switches it off, KSIG_STACK=1 on for any length.
   a.stack_len = 0;
   {
     const int st = env_int("KSIG_STACK", -1);
-    if (a.visit_per > 0 && mode == KSIG_PAIRS_FULL && pl.family == 0 && pl.diff && !pl.multi &&
-        LX >= 17 &&
-        (st > 0 || (st < 0 && LX <= 1024)))
+    if (a.visit_per > 0 && mode == KSIG_PAIRS_FULL && (pl.family == 0 || pl.family == 1) &&
+        pl.diff && !pl.multi && LX >= 17 && (st > 0 || (st < 0 && LX <= 1024)))
       a.stack_len = LX;
   }
+  // PDE: the column-major blocks alone were 1-3 % slower than round-robin
+  // (512 x 512 pairs, L = 200, dyadic 0 and 1); they stay only where the
+  // pairs stack.
+  if (pl.family == 1 && a.stack_len == 0) a.visit_per = 0;
   a.kind = kind;
   a.sp = sp;
   a.ralpha = (T)rbf_alpha(kind, param);

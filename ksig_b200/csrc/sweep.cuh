@@ -129,6 +129,7 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
   // columns, m = 10 went from 0 to 210 bytes of spills with them).
   constexpr bool kStackable = DIFF && !GIN && Policy::kStack && KD <= 12;
   const bool stack_on = kStackable && args.stack_len > 0 && args.visit_per > 0;
+  if constexpr (kStackable) pol.set_stack(stack_on ? args.stack_len : 0, args.nY);
 
   const int lane = threadIdx.x & 31;
   const long long wg = (long long)blockIdx.x * WPB + (threadIdx.x >> 5);
@@ -438,7 +439,7 @@ __device__ __forceinline__ void sweep(const SweepArgs<T>& args, Policy& pol,
         pol.fold_pair(nf, lane);
         ++nf;
       }
-      if (stack_on && __shfl_sync(FULL, pbnd ? 1 : 0, 31)) {
+      if (Policy::kCollect && stack_on && __shfl_sync(FULL, pbnd ? 1 : 0, 31)) {
         const long long q = (long long)__shfl_sync(FULL, nf, 31) - 1;
         const int t = __shfl_sync(FULL, pit.task + ((pr + 1) / args.stack_len - 1) * args.nY, 31);
         pol.collect(q, t, lane);
@@ -704,6 +705,9 @@ struct DpPolicy {
   // only: the order-p state leaves no registers for the stacking counters
   // (d = 16, 4 columns, m = 8, p = 2 spilled 116 bytes with them).
   static constexpr bool kStack = P == 1;
+  // Stacked pairs end in a warp-wide reduction of their level totals.
+  static constexpr bool kCollect = true;
+  __device__ void set_stack(int, int) {}
   T X[NX];                    // horizontal running sums (outgoing)
   T Ccol[NX][C];              // column running sums
   T Clast[C];                 // column sums of the last level's totals
@@ -937,7 +941,15 @@ struct PdePolicy {
   static constexpr int NX = 2 * F;
   static constexpr bool kUnroll2 = C * F <= 16 && sizeof(T) == 4;
   static constexpr bool kPairArg = false;
-  static constexpr bool kStack = false;
+  // Stacked pairs (SweepArgs::stack_len): at a separator row the lane resets
+  // its K values to the boundary value 1, on which the separator row (Z = 0)
+  // is a no-op that hands on the boundary values (1, 0); each pair's far
+  // corner is captured in row() as its cell row comes by.
+  static constexpr bool kStack = true;
+  static constexpr bool kCollect = false;
+  int slen = 0, tstride = 0;  // stacked sequence length, task stride (nY)
+  __device__ void set_stack(int len, int stride) { slen = len; tstride = stride; }
+  __device__ void fold_pair(long long, int) { begin_item(); }
   static constexpr int STRIP = DIFF ? 32 * C - 1 : 32 * C;
   T X[NX];
   T Kr[C * F];
@@ -965,7 +977,9 @@ struct PdePolicy {
       if (lane == 0) out[it.task] = 1.0;  // no cells: boundary value
       return;
     }
-    tgt_r = lx - 1;
+    // Far corner of the first (or only) pair; a stacked item's later pairs
+    // follow slen rows apart (row()).
+    tgt_r = slen > 0 ? slen - 2 : lx - 1;
     const int col = ly - 1;
     tgt_s = col / STRIP;
     const int rem = col - tgt_s * STRIP;
@@ -1021,7 +1035,12 @@ struct PdePolicy {
 #pragma unroll
       for (int c = 0; c < C; ++c)
         captured = fma(T(c == tgt_c ? 1 : 0), Kr[c * F + F - 1], captured);
-      out[it.task] = (double)captured;
+      if (slen > 0) {  // pair r / slen of a stacked item; the next corner
+        out[it.task + (r / slen) * tstride] = (double)captured;
+        tgt_r += slen;
+      } else {
+        out[it.task] = (double)captured;
+      }
     }
   }
   __device__ void end_item() {}
@@ -1070,6 +1089,7 @@ struct GaPolicy {
   static constexpr bool kUnroll2 = false;
   static constexpr bool kPairArg = false;
   static constexpr bool kStack = false;
+  static constexpr bool kCollect = false;
   static constexpr int STRIP = 32 * C;
   T X[NX];
   T Kr[C];       // logK of the row above, the lane's columns

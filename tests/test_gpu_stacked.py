@@ -139,3 +139,35 @@ def test_stacked_pairs_bench_size(monkeypatch):
                               param=float(np.sqrt(8)))[0, 0]
     got = float(stacked[:, a * 512 + b].sum())
     assert abs(got - want) <= 1e-5 * abs(want)
+
+
+@pytest.mark.parametrize('dt', [torch.float32, torch.float64])
+@pytest.mark.parametrize('nx,lx,ny,ly,dyadic', [
+    (300, 17, 77, 50, 0),
+    (131, 33, 97, 120, 1),
+    (1000, 40, 3, 60, 0),
+])
+def test_stacked_pde_bit_identical(dt, nx, lx, ny, ly, dyadic, monkeypatch):
+  """Goursat PDE on full grids: stacked columns (the separator row resets
+  the lane's K values to the boundary value) against round-robin pairs, bit
+  for bit, and sampled pairs against the FP64 oracle."""
+  from ksig_b200 import _engine as E
+  from ksig_b200 import _lib as L
+  rng = np.random.default_rng(nx + ly + dyadic)
+  X = torch.tensor(_walks(rng, nx, lx, 3), dtype=dt, device='cuda')
+  Y = torch.tensor(_walks(rng, ny, ly, 3), dtype=dt, device='cuda')
+
+  def values(stack):
+    monkeypatch.setenv('KSIG_STACK', stack)
+    return E.pde_values(E.Seqs(X), E.Seqs(Y), L.PAIRS_FULL, dyadic, True, L.STATIC_RBF, 0.9)
+
+  ref = values('0')
+  stacked = values('1')
+  assert torch.equal(stacked, ref)
+  Xn, Yn = X.double().cpu().numpy(), Y.double().cpu().numpy()
+  for a, b in ((0, 0), (nx - 1, ny - 1), (nx // 2, ny // 3)):
+    want = O.signature_pde_kernel(Xn[a:a + 1], Yn[b:b + 1], normalize=False,
+                                  dyadic_order=dyadic, param=0.9)[0, 0]
+    got = float(stacked[a * ny + b])
+    tol = 1e-4 if dt == torch.float32 else 1e-10
+    assert abs(got - want) <= tol * abs(want)
