@@ -146,6 +146,7 @@ def test_stacked_pairs_bench_size(monkeypatch):
     (300, 17, 77, 50, 0),
     (131, 33, 97, 120, 1),
     (1000, 40, 3, 60, 0),
+    (200, 20, 60, 45, 2),
 ])
 def test_stacked_pde_bit_identical(dt, nx, lx, ny, ly, dyadic, monkeypatch):
   """Goursat PDE on full grids: stacked columns (the separator row resets
