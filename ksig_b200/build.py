@@ -170,6 +170,10 @@ def instances():
   # with at least two levels (same tile, same records).
   out += [('dpr',) + inst[1:] for inst in out
           if inst[0] == 'dpb' and inst[5] == 1 and inst[4] >= 2]
+  # PDE forward with stacked pairs (equal-length full grids), for the tiles
+  # the sweep stacks (differencing, up to 12 coordinates).
+  out += [('pdes',) + inst[1:] for inst in out
+          if inst[0] == 'pde' and inst[6] == 1 and 0 < inst[2] <= 12]
   return out
 
 
@@ -178,6 +182,7 @@ OPS = {
     'pde': ('OP_PDE_FWD', 'pde_fwd_kernel<{T}, {kd}, {c}, {p}, {diff}, {wpb}, false>'),
     'dpx': ('OP_DP_FWD_EXT', 'dp_fwd_kernel<{T}, {kd}, {c}, {nl}, {p}, {diff}, {wpb}, true>'),
     'pdex': ('OP_PDE_FWD_EXT', 'pde_fwd_kernel<{T}, {kd}, {c}, {p}, {diff}, {wpb}, true>'),
+    'pdes': ('OP_PDE_FWD_STACK', 'pde_fwd_kernel<{T}, {kd}, {c}, {p}, {diff}, {wpb}, false, true>'),
     'ga': ('OP_GA_FWD', 'ga_fwd_kernel<{T}, {kd}, {c}, {wpb}>'),
     'dpb': ('OP_DP_BWD', 'dp_bwd_kernel<{T}, {kd}, {c}, {nl}, {p}, {wpb}>'),
     'dpr': ('OP_DP_REC_FWD', 'dp_rec_fwd_kernel<{T}, {kd}, {c}, {nl}, {p}, {wpb}>'),
@@ -187,7 +192,7 @@ OPS = {
 
 
 HEADER = {'dp': 'sweep.cuh', 'pde': 'sweep.cuh', 'dpx': 'sweep.cuh',
-          'pdex': 'sweep.cuh', 'ga': 'sweep.cuh', 'dpb': 'dp_bwd.cuh',
+          'pdex': 'sweep.cuh', 'pdes': 'sweep.cuh', 'ga': 'sweep.cuh', 'dpb': 'dp_bwd.cuh',
           'dpr': 'dp_bwd.cuh', 'dpc': 'dp_bwd.cuh', 'pdeb': 'pde_bwd.cuh'}
 
 

@@ -345,7 +345,6 @@ int plan_fwd(int family, int nX, int LX, int nY, int LY, int d, int dtype, int n
              FwdPlan& pl, bool allow_order = true, bool ext = false,
              bool layout_only = false) {
   const bool pde = family == 1, ga = family == 2;
-  pl.family = family;
   if (dtype != KSIG_DTYPE_F32 && dtype != KSIG_DTYPE_F64)
     return fail(KSIG_ERR_INVALID, "dtype must be KSIG_DTYPE_F32 or KSIG_DTYPE_F64");
   if (nX <= 0 || LX <= 0 || d <= 0) return fail(KSIG_ERR_INVALID, "empty X (n=%d, L=%d, d=%d)", nX, LX, d);
@@ -355,6 +354,7 @@ int plan_fwd(int family, int nX, int LX, int nY, int LY, int d, int dtype, int n
   const long long np = num_pairs(pairs_mode, nX, nY, n_list);
   if (np < 0 || np > (long long)0x7fffffff) return fail(KSIG_ERR_INVALID, "pair count %lld out of range", np);
   pl = FwdPlan{};
+  pl.family = family;
   pl.f64 = dtype == KSIG_DTYPE_F64;
   pl.diff = difference ? 1 : 0;
   pl.ntasks = np;
@@ -566,10 +566,21 @@ int run_fwd(const FwdPlan& pl, const void* X, const int32_t* lenX, int nX, int L
         pl.diff && !pl.multi && LX >= 17 && (st > 0 || (st < 0 && LX <= 1024)))
       a.stack_len = LX;
   }
-  // PDE: the column-major blocks alone were 1-3 % slower than round-robin
-  // (512 x 512 pairs, L = 200, dyadic 0 and 1); they stay only where the
-  // pairs stack.
-  if (pl.family == 1 && a.stack_len == 0) a.visit_per = 0;
+  // PDE: stacked pairs run in kernels of their own (OP_PDE_FWD_STACK, the
+  // same tile); without one the call does not stack.  Column-major blocks
+  // without stacking: 24.1 -> 21.6 ms with one strip per pair (512 x 512
+  // pairs, L = 200, 8 columns), but 1-3 % slower with two strips (4
+  // columns), where every strip reloads its column points anyway.
+  const void* func = pl.k->func;
+  if (pl.family == 1 && a.stack_len > 0) {
+    const KernelEntry* ks = find_kernel(OP_PDE_FWD_STACK, pl.f64, pl.k->kd, pl.c, 0, pl.p, 1);
+    if (ks && ks->kd == pl.k->kd && ks->c == pl.c && ks->p == pl.p && ks->wpb == pl.k->wpb &&
+        ensure_smem_attr(ks->func, pl.dyn_smem) == cudaSuccess)
+      func = ks->func;
+    else
+      a.stack_len = 0;
+  }
+  if (pl.family == 1 && a.stack_len == 0 && pl.multi) a.visit_per = 0;
   a.kind = kind;
   a.sp = sp;
   a.ralpha = (T)rbf_alpha(kind, param);
@@ -583,7 +594,7 @@ int run_fwd(const FwdPlan& pl, const void* X, const int32_t* lenX, int nX, int L
   a.status = status;
   void* kargs[] = {&a};
   if (!pl.gin) {
-    KSIG_CUDA(launch_main(pl.k->func, dim3(pl.grid), dim3(pl.k->wpb * 32), kargs, pl.dyn_smem, st));
+    KSIG_CUDA(launch_main(func, dim3(pl.grid), dim3(pl.k->wpb * 32), kargs, pl.dyn_smem, st));
     return KSIG_OK;
   }
   // Gram input: per chunk of tasks, the Gram slots, then the sweep on them.

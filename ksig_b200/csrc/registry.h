@@ -16,6 +16,7 @@ enum KernelOp : int {
   OP_GA_FWD = 6,       // SweepArgs<T>      ga_fwd_kernel (global alignment)
   OP_DP_REC_FWD = 7,   // DpBwdArgs<T>      dp_rec_fwd_kernel (split gradient pass)
   OP_DP_BWD_CKPT = 8,  // DpBwdArgs<T>      dp_bwd_ckpt_kernel (strip checkpointing)
+  OP_PDE_FWD_STACK = 9,  // SweepArgs<T>    pde_fwd_kernel, stacked pairs (STK)
 };
 
 struct KernelEntry {

@@ -936,16 +936,19 @@ dp_fwd_kernel(const SweepArgs<T> args) {
 // (the plain form loses ~3e-4 relative on 600 x 500 refined grids; this form
 // stays near 1e-6).  Exchange values per refined row: K and H at the lane's
 // right boundary.
-template <typename T, int C, int F, bool DIFF>
+template <typename T, int C, int F, bool DIFF, bool STK = false>
 struct PdePolicy {
   static constexpr int NX = 2 * F;
   static constexpr bool kUnroll2 = C * F <= 16 && sizeof(T) == 4;
   static constexpr bool kPairArg = false;
-  // Stacked pairs (SweepArgs::stack_len): at a separator row the lane resets
-  // its K values to the boundary value 1, on which the separator row (Z = 0)
-  // is a no-op that hands on the boundary values (1, 0); each pair's far
-  // corner is captured in row() as its cell row comes by.
-  static constexpr bool kStack = true;
+  // Stacked pairs (SweepArgs::stack_len, the STK instantiations): at a
+  // separator row the lane resets its K values to the boundary value 1, on
+  // which the separator row (Z = 0) is a no-op that hands on the boundary
+  // values (1, 0); each pair's far corner is captured in row() as its cell
+  // row comes by.  The stacking checks cost the PDE's light per-cell work
+  // 7.6 % on calls that cannot stack (ragged 256 x 256 pairs, L 64-512,
+  // dyadic 1: 14.4 -> 15.5 ms), hence kernels of their own.
+  static constexpr bool kStack = STK;
   static constexpr bool kCollect = false;
   int slen = 0, tstride = 0;  // stacked sequence length, task stride (nY)
   __device__ void set_stack(int len, int stride) { slen = len; tstride = stride; }
@@ -1048,13 +1051,13 @@ struct PdePolicy {
   __device__ void collect(long long, int, int) {}
 };
 
-template <typename T, int KD, int C, int F, bool DIFF, int WPB, bool EXT>
+template <typename T, int KD, int C, int F, bool DIFF, int WPB, bool EXT, bool STK = false>
 __global__ void __launch_bounds__(WPB * 32)
 pde_fwd_kernel(const SweepArgs<T> args) {
   __shared__ ItemMeta<T> ring[WPB][kItemRing];
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   auto* sm = reinterpret_cast<SweepSmem<T, KD, C>*>(dyn_smem);
-  PdePolicy<T, C, F, DIFF> pol;
+  PdePolicy<T, C, F, DIFF, STK> pol;
   pol.init(args.out);
   sweep<T, KD, C, DIFF, WPB, EXT>(args, pol, sm[threadIdx.x >> 5], ring[threadIdx.x >> 5]);
 }
