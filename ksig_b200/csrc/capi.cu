@@ -572,6 +572,7 @@ int run_fwd(const FwdPlan& pl, const void* X, const int32_t* lenX, int nX, int L
   // pairs, L = 200, 8 columns), but 1-3 % slower with two strips (4
   // columns), where every strip reloads its column points anyway.
   const void* func = pl.k->func;
+  if (pl.family == 1 && pl.k->op != OP_PDE_FWD) a.stack_len = 0;  // EXT kinds: no stacked tiles
   if (pl.family == 1 && a.stack_len > 0) {
     const KernelEntry* ks = find_kernel(OP_PDE_FWD_STACK, pl.f64, pl.k->kd, pl.c, 0, pl.p, 1);
     if (ks && ks->kd == pl.k->kd && ks->c == pl.c && ks->p == pl.p && ks->wpb == pl.k->wpb &&

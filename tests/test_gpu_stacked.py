@@ -172,3 +172,28 @@ def test_stacked_pde_bit_identical(dt, nx, lx, ny, ly, dyadic, monkeypatch):
     got = float(stacked[a * ny + b])
     tol = 1e-4 if dt == torch.float32 else 1e-10
     assert abs(got - want) <= tol * abs(want)
+
+
+@pytest.mark.parametrize('static', ['matern32', 'poly'])
+def test_pde_other_static_kernels_full_grid(static, monkeypatch):
+  """PDE K(X, Y) on a full grid of equal-length sequences with the other
+  static kernels (their own sweep instantiations, which have no stacked
+  form): the same values with and without stacking enabled, and the FP64
+  oracle on sampled pairs."""
+  import ksig_b200 as K
+  sk = {'matern32': lambda: K.Matern32Kernel(1.3),
+        'poly': lambda: K.PolynomialKernel(degree=2, gamma=0.5, scale=1.0)}[static]()
+  rng = np.random.default_rng(29)
+  X = _walks(rng, 200, 24, 3)
+  Y = _walks(rng, 41, 30, 3)
+  kern = K.SignaturePDEKernel(normalize=False, static_kernel=sk, dyadic_order=0)
+  monkeypatch.setenv('KSIG_STACK', '0')
+  ref = kern(X, Y)
+  monkeypatch.setenv('KSIG_STACK', '1')
+  got = kern(X, Y)
+  assert np.array_equal(got, ref)
+  param = {'matern32': 1.3, 'poly': (2, 0.5, 1.0)}[static]
+  for a, b in ((0, 0), (199, 40), (77, 13)):
+    want = O.signature_pde_kernel(X[a:a + 1], Y[b:b + 1], normalize=False, kind=static,
+                                  param=param, dyadic_order=0)[0, 0]
+    assert abs(got[a, b] - want) <= 1e-9 * abs(want)
